@@ -1,0 +1,345 @@
+#!/usr/bin/env python
+"""Throughput of the MCML photon-transport hot path on B200.
+
+One step = one pass of the hot path over the 5-layer benchmark tissue
+(tests/golden/configs/c1: heights 0.3/0.7/0.2/0.4/semi-infinite cm,
+mua ~ U(0.05,0.5)/cm, mus ~ U(50,250)/cm drawn by seed, g=0.9, n=1.4,
+three oblique fibres at 0.8/1.5/3.0 cm): walk 1e8 photons, then replay
+every detected photon with per-layer pathlengths and the A_rz / A0_z
+tallies (the reference's `-R -A -B` path).  Metric: photons/s.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mcml|reference]
+
+`value` times the device pipeline with inputs resident (CUDA events on the
+launching stream, L2 flushed between steps); `e2e` times the same work
+through the public API from host structs to host result buffers.  The
+reference arm (`--impl reference`) times the CPU restatement of the
+reference algorithm (the reference has no CPU implementation) on all host
+cores over a bounded photon sample.  Under torchrun each rank walks its
+own subsequence range (weak scaling) and rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+CONFIG = ROOT / "tests" / "golden" / "configs" / "c1"
+METRIC = "photons/s (plain MC)"
+WORKLOAD = "plain MC + replay, 5-layer tissue, 1e8 photons, -R -A -B (config 1)"
+
+# Per-step work of the walk, counted by hand from the step's arithmetic
+# (hop + drop + Henyey-Greenstein spin + roulette test, the path a step
+# takes when it neither crosses a boundary nor plays roulette):
+#   XORWOW draw: 9 integer ops + 1 convert + 1 FMA; 3 draws per step.
+#   FP32/INT32 lane ops per step ........................ OPS_LANE
+#   quarter-rate ops (MUFU lg2/rcp/sin/cos/rsqrt/sqrt, and
+#   int<->float conversions) per step ................... OPS_XU
+# B200 SM per clock: 128 FP32 lanes, 16 MUFU/conversion lanes.
+OPS_LANE = 118
+OPS_XU = 15
+SM_COUNT = 148
+
+
+def steps_per_clock_per_sm() -> float:
+    return min(128.0 / OPS_LANE, 16.0 / OPS_XU)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+        self._t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self._t = threading.Thread(target=self._read, daemon=True)
+        self._t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self._t:
+            self._t.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        load = [v for v in sm if v > 0]
+        return {"sm_mhz": statistics.median(load) if load else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def load_sim(photons: int | None):
+    import mcml_gpu_b200 as m
+    sim = m.parse_config(CONFIG / "sim_set.json", CONFIG / "input.txt")[0]
+    if photons:
+        sim.number_photons = int(photons)
+    return sim
+
+
+def cpu_port_rate(sim, seconds: float, threads: int = 0) -> dict:
+    """The CPU restatement (oracle, FP32, PCG32) timed on all host cores over a
+    photon sample sized to take about `seconds`."""
+    import oracle
+    pilot = 2000
+    t0 = time.perf_counter()
+    oracle.run(sim, pilot, 99, first=10**12, threads=threads)
+    dt = max(time.perf_counter() - t0, 1e-3)
+    n = max(pilot, int(pilot * seconds / dt))
+    t0 = time.perf_counter()
+    st, *_ = oracle.run(sim, n, 7, first=0, threads=threads)
+    dt = time.perf_counter() - t0
+    cores = threads if threads > 0 else (os.cpu_count() or 1)
+    return {"value": n / dt, "unit": "photons/s", "cores": cores, "kind": "port",
+            "sample": f"{n} photons of the benchmark tissue (first pass, FP32, PCG32 per photon), "
+                      f"{dt:.1f} s on {cores} threads; {st.steps / max(st.photons, 1):.1f} steps/photon"}
+
+
+def reference_arm(args) -> int:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    sim = load_sim(args.photons)
+    cores = os.cpu_count() or 1
+    # each step: a bounded sample of the workload on all cores
+    import oracle
+    sample = args.ref_sample
+    for _ in range(args.warmup):
+        oracle.run(sim, max(sample // 10, 1000), 3, first=10**12)
+    times = []
+    steps = 0
+    for k in range(args.steps):
+        t0 = time.perf_counter()
+        st, *_ = oracle.run(sim, sample, 1000 + k)
+        times.append(time.perf_counter() - t0)
+        steps += st.steps
+    total = sum(times)
+    value = sample * args.steps / total
+    line = {
+        "metric": METRIC, "value": value, "unit": "photons/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "impl": "reference",
+        "config": {"workload": WORKLOAD, "photons_per_step": sample, "note":
+                   "CPU restatement of the reference walk (the reference has no CPU path)"},
+        "cpu_baseline": {"value": value, "unit": "photons/s", "cores": cores, "kind": "port",
+                         "sample": f"{sample} photons per step, FP32, {cores} threads, "
+                                   f"{steps / (sample * args.steps):.1f} steps/photon"},
+        "e2e": {"value": value, "unit": "photons/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def read_traffic() -> float | None:
+    p = ROOT / "profiles" / "walk_kernel_traffic.json"
+    if not p.exists():
+        return None
+    try:
+        return float(json.loads(p.read_text())["dram_bytes_per_launch"])
+    except Exception:
+        return None
+
+
+def mcml_arm(args) -> int:
+    import torch
+    import mcml_gpu_b200 as m
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    sim = load_sim(args.photons)
+    N = int(sim.number_photons)
+    info = m.device_info(local)
+    slots = args.slots or int(info.reference_threads)
+    stream = torch.cuda.current_stream()
+    run = m.Simulation(sim, seed=args.seed + rank, slots=slots, slot_begin=rank * slots,
+                       device=local, stream=stream.cuda_stream, block_size=args.block,
+                       blocks_per_sm=args.blocks_per_sm)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+
+    def step():
+        run.launch_run()
+        run.launch_replay()
+
+    for _ in range(args.warmup):
+        flush.zero_()
+        step()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    walk_ms = []
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    wall0 = time.perf_counter()
+    for k in range(args.steps):
+        flush.zero_()
+        starts[k].record(stream)
+        step()
+        ends[k].record(stream)
+        res = None
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - wall0
+    if dist:
+        dist.barrier()
+    clocks = sampler.stop()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    res = run.result()  # the last step's first pass
+    rep = run.replay()  # (re-runs the replay once, outside the timed region, for the row count)
+    total_ms = sum(step_ms)
+    if dist:
+        t = torch.tensor([total_ms], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * N * args.steps / (total_ms / 1000.0)
+
+    # e2e through the public API: host struct in, host rows and tallies out
+    e2e_steps = max(1, min(args.steps, 3))
+    L, S = sim.num_layers, sim.num_sds
+    nr, nz = 1000, 500
+    arz = np.empty((S, nz, nr), dtype=np.uint64)
+    d2h = 0
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        run.set_sim(sim)
+        r1 = run.run()
+        r2 = run.replay()
+        nrows = 0
+        for sds in range(1, S + 1):
+            rows, inter = run.rows(sds)
+            nrows += rows.shape[0]
+        a_rz, a0_z = run.tallies()
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if dist:
+        t = torch.tensor([e2e_s], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    d2h = (m.C.sizeof(m.Result) * 2 + nrows * ((L + 2) * 4 + L * 4) + 12 * nrows
+           + a_rz.nbytes + a0_z.nbytes)
+    h2d = m.C.sizeof(m.Sim)
+
+    steps_per_photon = res.steps / max(res.photons, 1)
+    walk_kernel_ms = float(res.walk_ms)
+    achieved = res.steps / (walk_kernel_ms / 1000.0)
+    f_sm = clocks.get("sm_mhz") or 1965.0
+    peak = f_sm * 1e6 * info.sm_count * steps_per_clock_per_sm()
+    line = {
+        "metric": METRIC, "value": value, "unit": "photons/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "photons": N, "layers": L, "sds": S,
+                   "grid": "1000x500 @ 0.01 cm", "slots": slots,
+                   "l2": "flushed between steps (256 MiB write)",
+                   "parallelism": f"replicas x{world}, disjoint RNG subsequences",
+                   "steps_per_photon": round(steps_per_photon, 2),
+                   "detected": [int(v) for v in res.detected[:S]],
+                   "replayed_rows": int(sum(rep.detected[:S]))},
+        "e2e": {"value": N * world / e2e_s, "unit": "photons/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": 4 * args.steps,
+        "roofline": {"bound": "issue", "achieved": achieved / 1e9, "peak": peak / 1e9,
+                     "unit": "Gstep/s", "frac": achieved / peak,
+                     "traffic": read_traffic(),
+                     "kernel": "walk_kernel",
+                     "model": f"steps/s <= f_sm x {info.sm_count} SMs x min(128/{OPS_LANE}, "
+                              f"16/{OPS_XU}) at the measured median SM clock",
+                     "walk_ms": walk_kernel_ms, "seed_ms": float(res.seed_ms),
+                     "replay_ms": float(rep.replay_ms)},
+        "clocks": clocks,
+        "wall_s_timed": wall,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_port_rate(load_sim(None), args.cpu_seconds)
+    run.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["mcml", "reference"], default="mcml")
+    ap.add_argument("--photons", type=int, default=0, help="override N (default: 1e8)")
+    ap.add_argument("--slots", type=int, default=0)
+    ap.add_argument("--block", type=int, default=0)
+    ap.add_argument("--blocks-per-sm", type=int, default=0)
+    ap.add_argument("--seed", type=int, default=1234)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-sample", type=int, default=300000)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return reference_arm(args)
+    return mcml_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,251 @@
+/*
+ * mcml_b200.h -- C ABI of the B200-native MCML photon-transport library.
+ *
+ * The reference (MCML_GPU K3.02) has no library boundary: its CLI, host
+ * driver and kernels share one process and a set of global __constant__
+ * symbols.  This header is the seam a maintainer of that code base would
+ * bind to instead.  Every entry point names the reference function(s) it
+ * replaces as file:line of the reference project.
+ *
+ * Conventions
+ *  - Every call returns MCML_OK (0) or a negative mcml_status.  Nothing is
+ *    printed by the library; mcml_last_error() holds a message for the
+ *    calling thread.
+ *  - The caller owns every struct and host array passed in.  The library
+ *    owns the device buffers of an mcml_ctx and frees them in mcml_destroy.
+ *  - An mcml_ctx holds one simulation's parameter block (the reference's
+ *    __constant__ tables, header.h:205-214) and its device buffers.  Use
+ *    one context per host thread or stream; contexts share no state.
+ *  - Weights are in the reference's units: an integer number of quanta of
+ *    1/0xFFFFFFFF of a launched photon, held in float (header.h:95).
+ */
+#ifndef MCML_B200_H
+#define MCML_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Limits of the reference: PRESET_NUM_LAYER and PRESET_NUM_DETECTOR (header.h:38,44). */
+#define MCML_MAX_LAYERS 10
+#define MCML_MAX_SDS 30
+
+/* Absorbance grid of the reference: record_nr/nz/dr/dz (header.h:65-68). */
+#define MCML_REF_GRID_NR 1000
+#define MCML_REF_GRID_NZ 500
+#define MCML_REF_GRID_D 0.01f
+
+typedef enum mcml_status {
+  MCML_OK = 0,
+  MCML_E_INVALID = -1,  /* bad argument or configuration value        */
+  MCML_E_CUDA = -2,     /* a CUDA runtime call failed                  */
+  MCML_E_NOMEM = -3,    /* host or device allocation failed            */
+  MCML_E_OVERFLOW = -4, /* detection-record buffer too small           */
+  MCML_E_IO = -5,       /* file could not be opened or written         */
+  MCML_E_PARSE = -6,    /* sim_set.json / input.txt could not be read  */
+  MCML_E_STATE = -7,    /* calls made in the wrong order               */
+  MCML_E_BUDGET = -8,   /* a kernel hit its step budget and stopped    */
+  MCML_E_NODEV = -9     /* no CUDA device                              */
+} mcml_status;
+
+/*
+ * One simulation: the fields of sim_set.json plus one line of input.txt,
+ * already converted to the types the reference stores them in
+ * (io.cpp:48-191 for the JSON keys, io.cpp:138-147 for input.txt).
+ * Angles are in degrees, as in the file; the library converts them with
+ * the reference's float arithmetic (io.cpp:184,190).
+ */
+typedef struct mcml_sim {
+  uint64_t number_photons;      /* "number_photons"                         */
+  uint32_t num_layers;          /* "number_layers" (1..MCML_MAX_LAYERS)     */
+  uint32_t num_sds;             /* "probes.num_SDS" (1..MCML_MAX_SDS)       */
+  float upper_n;                /* "upper_n"                                */
+  float lower_n;                /* "lower_n"                                */
+  float detector_reflectance;   /* "detector_reflectance" in [0,1]          */
+  int32_t source_probe_oblique; /* 1: pencil beam at "angle"; 0: disc+cone  */
+  int32_t detector_probe_oblique; /* 1: oblique fibre ovals; 0: rings       */
+  float source_NA;
+  float source_radius;          /* cm                                       */
+  float source_angle_deg;
+  float det_pos[MCML_MAX_SDS];       /* cm from the source centre           */
+  float det_NA[MCML_MAX_SDS];
+  float det_radius[MCML_MAX_SDS];    /* cm                                  */
+  float det_angle_deg[MCML_MAX_SDS];
+  float height[MCML_MAX_LAYERS];     /* cm; the last layer's value is unused */
+  float mua[MCML_MAX_LAYERS];        /* 1/cm                                */
+  float mus[MCML_MAX_LAYERS];        /* 1/cm                                */
+  float n[MCML_MAX_LAYERS];
+  float g[MCML_MAX_LAYERS];
+} mcml_sim;
+
+/* Run options.  Zero-initialise and set what you need. */
+typedef struct mcml_opts {
+  uint64_t seed;            /* XORWOW seed (reference: time(NULL), transport.cu:72) */
+  uint64_t slots;           /* RNG subsequences ("photon slots"); 0 = the reference's
+                               thread count on this device, SMs x max threads/SM
+                               (io.cpp:522-526), so that slot t walks the photons the
+                               reference's thread t walks.  N==slots gives the
+                               reference's one-photon-per-thread layout.            */
+  int32_t device;           /* CUDA ordinal (reference: -G, main.cu:51-59)          */
+  uint32_t grid_nr;         /* absorbance grid; 0 = 1000                            */
+  uint32_t grid_nz;         /* 0 = 500                                              */
+  float grid_dr;            /* cm; 0 = 0.01                                         */
+  float grid_dz;            /* cm; 0 = 0.01                                         */
+  uint64_t record_capacity; /* detection records kept on the device; 0 = automatic  */
+  void *stream;             /* cudaStream_t to launch on; NULL = a library stream   */
+  uint32_t block_size;      /* threads per block of the walk; 0 = tuned default     */
+  uint32_t blocks_per_sm;   /* resident blocks per SM of the walk; 0 = tuned        */
+  uint64_t replay_step_budget; /* max steps of one replayed photon; 0 = 1<<26        */
+  uint64_t slot_begin;      /* first subsequence of this context: a shard of a
+                               multi-GPU run uses slot_begin = rank * slots          */
+} mcml_opts;
+
+/* Per-SDS result of the first pass (and, after mcml_replay, of the replay). */
+typedef struct mcml_result {
+  uint32_t num_sds;
+  uint64_t photons;                  /* photons walked                        */
+  uint64_t steps;                    /* walk steps (loop iterations)          */
+  uint64_t detected[MCML_MAX_SDS];   /* SDS_detected_number (io.cpp:374-378)  */
+  double weight_sum[MCML_MAX_SDS];   /* sum of detected weights, in quanta     */
+  double weight_sumsq[MCML_MAX_SDS]; /* sum of squared detected weights        */
+  double reflectance[MCML_MAX_SDS];  /* weight_sum / (0xFFFFFFFF * N) (io.cpp:16-28) */
+  double std_error[MCML_MAX_SDS];    /* standard error of reflectance[]       */
+  float walk_ms;                     /* device time of the walk kernel        */
+  float replay_ms;                   /* device time of the replay             */
+  float seed_ms;                     /* device time of the slot seeding       */
+} mcml_result;
+
+typedef struct mcml_device_info {
+  char name[100];
+  int32_t major, minor;
+  int32_t sm_count;
+  int32_t max_threads_per_sm;
+  uint64_t global_mem;
+  uint64_t reference_threads; /* the reference's autototalthread (io.cpp:522-526) */
+} mcml_device_info;
+
+typedef struct mcml_ctx mcml_ctx;
+
+/* ---- library ---------------------------------------------------------- */
+const char *mcml_version(void);
+const char *mcml_strerror(int status);
+/* Message of the last failing call on this thread (never NULL). */
+const char *mcml_last_error(void);
+
+/* Replaces list_GPU (io.cpp:495-544) for one device. */
+int mcml_device_count(int *count);
+int mcml_get_device_info(int device, mcml_device_info *info);
+
+/* ---- configuration ---------------------------------------------------- */
+/*
+ * Replaces read_mua_mus (io.cpp:35-256): reads sim_set.json and input.txt
+ * into up to max_sims mcml_sim structs.  Checks the same things the
+ * reference checks, with the same wording in mcml_last_error():
+ * oblique flags 0/1, detector_reflectance in [0,1], layer and SDS limits,
+ * detector count vs list size, and the last layer's mus>0, n>1, g<=1.
+ */
+int mcml_parse_config(const char *sim_json_path, const char *input_txt_path,
+                      mcml_sim *sims, int max_sims, int *num_sims);
+
+/* Derived per-simulation constants, computed exactly as io.cpp:168-238 does. */
+typedef struct mcml_derived {
+  float z_min[MCML_MAX_LAYERS + 2];
+  float z_max[MCML_MAX_LAYERS + 2];
+  float mutr[MCML_MAX_LAYERS + 2];  /* 1/(mua+mus)                       */
+  float start_weight;               /* (u32)(0xffffffff*(1-R_specular))  */
+  float critical_angle[MCML_MAX_SDS + 1]; /* asin(NA/upper_n), index 1..S */
+  float det_angle_rad[MCML_MAX_SDS + 1];  /* index 0 = source            */
+} mcml_derived;
+int mcml_derive(const mcml_sim *sim, mcml_derived *out);
+
+/* ---- simulation ------------------------------------------------------- */
+/* Replaces InitMemStructs + InitDCMem (transport.cu:1002-1070). */
+int mcml_create(const mcml_sim *sim, const mcml_opts *opts, mcml_ctx **ctx);
+/* Uploads a new parameter block to an existing context (same limits). */
+int mcml_set_sim(mcml_ctx *ctx, const mcml_sim *sim);
+void mcml_destroy(mcml_ctx *ctx);
+
+/*
+ * First pass: replaces LaunchPhoton_Global + the MCd launch loop +
+ * calculate_reflectance (transport.cu:106-147, 299-311).  Walks all
+ * photons in one persistent launch, keeps one record per detection on the
+ * device and returns per-SDS counts and weight sums.  Blocks until done.
+ */
+int mcml_run(mcml_ctx *ctx, mcml_result *result);
+/* Same work, enqueued on the context's stream without waiting. */
+int mcml_launch_run(mcml_ctx *ctx);
+
+/*
+ * Replay: replaces the per-SDS MCd_replay batches and
+ * calculate_reflectance_replay (transport.cu:160-222, 315-332).  Re-walks
+ * every detected photon from its saved XORWOW state, producing its row
+ * [weight, PL_1..PL_L, steps], per-layer interaction counts, and the A_rz /
+ * A0_z tallies.  Blocks until done; result (if non-NULL) gets the replayed
+ * weight sums.
+ */
+int mcml_replay(mcml_ctx *ctx, mcml_result *result);
+int mcml_launch_replay(mcml_ctx *ctx);
+
+/* Waits for the context's stream and fills result from the first pass. */
+int mcml_get_result(mcml_ctx *ctx, mcml_result *result);
+
+/*
+ * Detected photons of one SDS (1-based sds), ordered by photon index
+ * (slot-major), which is the reference's order when N equals its thread
+ * count.  photon_ids / weights may be NULL.  *count gets the number of rows.
+ */
+int mcml_get_detections(mcml_ctx *ctx, int sds, uint64_t *photon_ids,
+                        float *weights, uint64_t capacity, uint64_t *count);
+
+/*
+ * Replay rows of one SDS in the pathlength_SDS_#.bin layout (io.cpp:302-311):
+ * count rows of (L+2) float32 = weight, PL_1..PL_L [cm], steps.  Same order
+ * as mcml_get_detections.  interactions (may be NULL) gets count*L uint32
+ * per-layer scattering-event counts, which the reference does not record.
+ */
+int mcml_get_rows(mcml_ctx *ctx, int sds, float *rows, uint32_t *interactions,
+                  uint64_t capacity, uint64_t *count);
+
+/*
+ * Absorbance tallies after mcml_replay, in u64 weight quanta, laid out as
+ * the reference's A_rz[sds][iz][ir] and A0_z[sds][iz] (transport.cu:583-588).
+ * Either pointer may be NULL.
+ */
+int mcml_get_tallies(mcml_ctx *ctx, uint64_t *A_rz, uint64_t *A0_z);
+
+/* Replaces calculate_average_pathlength (transport.cu:274-297): out[S*L]. */
+int mcml_average_pathlength(mcml_ctx *ctx, double *out);
+
+/*
+ * Writes the reference's output files for one simulation, with the
+ * reference's names, modes and byte layouts (io.cpp:11-33, 281-469):
+ * output_txt (append), summary.json (append), and with replay,
+ * pathlength_SDS_#.{bin,txt}, average_pathlength.txt, A_rz_SDS_#.{bin,txt},
+ * A0_z_SDS_#.{bin,txt}, into directory dir ("" = current directory).
+ * flags: MCML_OUT_* below.  sim_s / replay_s go into summary.json.
+ */
+#define MCML_OUT_REPLAY 1u       /* -R  */
+#define MCML_OUT_ABSORBANCE 2u   /* -A  */
+#define MCML_OUT_PATHLENGTH 4u   /* -P  */
+#define MCML_OUT_AVERAGE_PL 8u   /* -AP */
+#define MCML_OUT_BINARY 16u      /* -B  */
+int mcml_write_outputs(mcml_ctx *ctx, const char *dir, const char *output_txt,
+                       uint32_t flags, double sim_s, double replay_s);
+
+/* ---- test support ------------------------------------------------------ */
+/*
+ * The first count draws of curand_uniform on the XORWOW state
+ * curand_init(seed, subsequence, 0) -- the stream the reference's thread
+ * `subsequence` consumes (transport.cu:51-55, 733).  Host output buffer.
+ * Used to feed recorded draws to the CPU oracle.
+ */
+int mcml_uniform_stream(int device, uint64_t seed, uint64_t subsequence,
+                        uint64_t count, float *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MCML_B200_H */

@@ -1,0 +1,393 @@
+"""mcml_gpu_b200 -- B200-native MCML photon transport (Python host mirror).
+
+The compute path is the CUDA library ``lib/libmcml_b200.so`` built from
+``csrc/`` for sm_100a (``python -m mcml_gpu_b200.build``).  This module binds
+its C ABI (``include/mcml_b200.h``) with ctypes and mirrors the reference's
+host flow (MCML_GPU K3.02, transport.cu:57-272): parse the configuration,
+run the first pass, replay the detected photons, write the output files.
+
+There is no CPU fallback: every call that computes goes through the CUDA
+library, and loading fails loudly when it has not been built.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+from pathlib import Path
+from typing import Optional, Sequence
+
+import numpy as np
+
+__all__ = [
+    "MAX_LAYERS", "MAX_SDS", "MCMLError", "Sim", "Opts", "Result", "Derived",
+    "DeviceInfo", "load_library", "lib_path", "parse_config", "derive", "make_sim",
+    "Simulation", "uniform_stream", "device_count", "device_info",
+    "OUT_REPLAY", "OUT_ABSORBANCE", "OUT_PATHLENGTH", "OUT_AVERAGE_PL", "OUT_BINARY",
+]
+
+MAX_LAYERS = 10
+MAX_SDS = 30
+OUT_REPLAY, OUT_ABSORBANCE, OUT_PATHLENGTH, OUT_AVERAGE_PL, OUT_BINARY = 1, 2, 4, 8, 16
+
+_PKG = Path(__file__).resolve().parent
+
+
+def lib_path() -> Path:
+    return _PKG / "lib" / "libmcml_b200.so"
+
+
+class MCMLError(RuntimeError):
+    def __init__(self, status: int, where: str, message: str):
+        super().__init__(f"{where}: status {status}: {message}")
+        self.status = status
+        self.message = message
+
+
+class Sim(C.Structure):
+    """mcml_sim: one simulation (sim_set.json fields + one input.txt line)."""
+    _fields_ = [
+        ("number_photons", C.c_uint64),
+        ("num_layers", C.c_uint32),
+        ("num_sds", C.c_uint32),
+        ("upper_n", C.c_float),
+        ("lower_n", C.c_float),
+        ("detector_reflectance", C.c_float),
+        ("source_probe_oblique", C.c_int32),
+        ("detector_probe_oblique", C.c_int32),
+        ("source_NA", C.c_float),
+        ("source_radius", C.c_float),
+        ("source_angle_deg", C.c_float),
+        ("det_pos", C.c_float * MAX_SDS),
+        ("det_NA", C.c_float * MAX_SDS),
+        ("det_radius", C.c_float * MAX_SDS),
+        ("det_angle_deg", C.c_float * MAX_SDS),
+        ("height", C.c_float * MAX_LAYERS),
+        ("mua", C.c_float * MAX_LAYERS),
+        ("mus", C.c_float * MAX_LAYERS),
+        ("n", C.c_float * MAX_LAYERS),
+        ("g", C.c_float * MAX_LAYERS),
+    ]
+
+
+class Opts(C.Structure):
+    _fields_ = [
+        ("seed", C.c_uint64),
+        ("slots", C.c_uint64),
+        ("device", C.c_int32),
+        ("grid_nr", C.c_uint32),
+        ("grid_nz", C.c_uint32),
+        ("grid_dr", C.c_float),
+        ("grid_dz", C.c_float),
+        ("record_capacity", C.c_uint64),
+        ("stream", C.c_void_p),
+        ("block_size", C.c_uint32),
+        ("blocks_per_sm", C.c_uint32),
+        ("replay_step_budget", C.c_uint64),
+        ("slot_begin", C.c_uint64),
+    ]
+
+
+class Result(C.Structure):
+    _fields_ = [
+        ("num_sds", C.c_uint32),
+        ("photons", C.c_uint64),
+        ("steps", C.c_uint64),
+        ("detected", C.c_uint64 * MAX_SDS),
+        ("weight_sum", C.c_double * MAX_SDS),
+        ("weight_sumsq", C.c_double * MAX_SDS),
+        ("reflectance", C.c_double * MAX_SDS),
+        ("std_error", C.c_double * MAX_SDS),
+        ("walk_ms", C.c_float),
+        ("replay_ms", C.c_float),
+        ("seed_ms", C.c_float),
+    ]
+
+    def as_dict(self) -> dict:
+        s = self.num_sds
+        return {
+            "photons": int(self.photons),
+            "steps": int(self.steps),
+            "detected": [int(v) for v in self.detected[:s]],
+            "weight_sum": list(self.weight_sum[:s]),
+            "weight_sumsq": list(self.weight_sumsq[:s]),
+            "reflectance": list(self.reflectance[:s]),
+            "std_error": list(self.std_error[:s]),
+            "walk_ms": float(self.walk_ms),
+            "replay_ms": float(self.replay_ms),
+        }
+
+
+class Derived(C.Structure):
+    _fields_ = [
+        ("z_min", C.c_float * (MAX_LAYERS + 2)),
+        ("z_max", C.c_float * (MAX_LAYERS + 2)),
+        ("mutr", C.c_float * (MAX_LAYERS + 2)),
+        ("start_weight", C.c_float),
+        ("critical_angle", C.c_float * (MAX_SDS + 1)),
+        ("det_angle_rad", C.c_float * (MAX_SDS + 1)),
+    ]
+
+
+class DeviceInfo(C.Structure):
+    _fields_ = [
+        ("name", C.c_char * 100),
+        ("major", C.c_int32),
+        ("minor", C.c_int32),
+        ("sm_count", C.c_int32),
+        ("max_threads_per_sm", C.c_int32),
+        ("global_mem", C.c_uint64),
+        ("reference_threads", C.c_uint64),
+    ]
+
+
+_lib: Optional[C.CDLL] = None
+
+# (name, restype, argtypes) of every entry point of include/mcml_b200.h
+_SIGNATURES = [
+    ("mcml_version", C.c_char_p, []),
+    ("mcml_strerror", C.c_char_p, [C.c_int]),
+    ("mcml_last_error", C.c_char_p, []),
+    ("mcml_device_count", C.c_int, [C.POINTER(C.c_int)]),
+    ("mcml_get_device_info", C.c_int, [C.c_int, C.POINTER(DeviceInfo)]),
+    ("mcml_parse_config", C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(Sim), C.c_int,
+                                    C.POINTER(C.c_int)]),
+    ("mcml_derive", C.c_int, [C.POINTER(Sim), C.POINTER(Derived)]),
+    ("mcml_create", C.c_int, [C.POINTER(Sim), C.POINTER(Opts), C.POINTER(C.c_void_p)]),
+    ("mcml_set_sim", C.c_int, [C.c_void_p, C.POINTER(Sim)]),
+    ("mcml_destroy", None, [C.c_void_p]),
+    ("mcml_run", C.c_int, [C.c_void_p, C.POINTER(Result)]),
+    ("mcml_launch_run", C.c_int, [C.c_void_p]),
+    ("mcml_replay", C.c_int, [C.c_void_p, C.POINTER(Result)]),
+    ("mcml_launch_replay", C.c_int, [C.c_void_p]),
+    ("mcml_get_result", C.c_int, [C.c_void_p, C.POINTER(Result)]),
+    ("mcml_get_detections", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                      C.c_uint64, C.POINTER(C.c_uint64)]),
+    ("mcml_get_rows", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_uint64,
+                                C.POINTER(C.c_uint64)]),
+    ("mcml_get_tallies", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("mcml_average_pathlength", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("mcml_write_outputs", C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_uint32,
+                                     C.c_double, C.c_double]),
+    ("mcml_uniform_stream", C.c_int, [C.c_int, C.c_uint64, C.c_uint64, C.c_uint64,
+                                      C.c_void_p]),
+]
+
+
+def exported_symbols() -> list[str]:
+    """Entry points this module binds (all of include/mcml_b200.h)."""
+    return [s[0] for s in _SIGNATURES]
+
+
+def load_library() -> C.CDLL:
+    """Load the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = lib_path()
+    if not p.exists():
+        raise ImportError(f"{p} is missing: build it with `python -m mcml_gpu_b200.build`")
+    lib = C.CDLL(str(p))
+    for name, res, args in _SIGNATURES:
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _check(rc: int, where: str) -> None:
+    if rc != 0:
+        lib = load_library()
+        raise MCMLError(rc, where, lib.mcml_last_error().decode(errors="replace"))
+
+
+def device_count() -> int:
+    lib = load_library()
+    n = C.c_int(0)
+    rc = lib.mcml_device_count(C.byref(n))
+    return n.value if rc == 0 else 0
+
+
+def device_info(device: int = 0) -> DeviceInfo:
+    lib = load_library()
+    info = DeviceInfo()
+    _check(lib.mcml_get_device_info(device, C.byref(info)), "mcml_get_device_info")
+    return info
+
+
+def parse_config(sim_json: os.PathLike | str, input_txt: os.PathLike | str) -> list[Sim]:
+    """read_mua_mus (io.cpp:35-256): returns one Sim per simulation."""
+    lib = load_library()
+    n = C.c_int(0)
+    _check(lib.mcml_parse_config(str(sim_json).encode(), str(input_txt).encode(), None, 0,
+                                 C.byref(n)), "mcml_parse_config")
+    arr = (Sim * n.value)()
+    _check(lib.mcml_parse_config(str(sim_json).encode(), str(input_txt).encode(), arr, n.value,
+                                 C.byref(n)), "mcml_parse_config")
+    return list(arr)
+
+
+def derive(sim: Sim) -> Derived:
+    lib = load_library()
+    d = Derived()
+    _check(lib.mcml_derive(C.byref(sim), C.byref(d)), "mcml_derive")
+    return d
+
+
+def make_sim(layers: Sequence[Sequence[float]], detectors: Sequence[Sequence[float]], *,
+             photons: int, upper_n: float = 1.457, lower_n: float = 1.457,
+             detector_reflectance: float = 0.0, source_oblique: bool = True,
+             detector_oblique: bool = True, source: Sequence[float] = (0.37, 0.075, 0.0)) -> Sim:
+    """Builds a Sim.  layers: (height, mua, mus, n, g) per layer, the last
+    layer's height ignored.  detectors: (pos, NA, radius, angle_deg).
+    source: (NA, radius, angle_deg)."""
+    s = Sim()
+    s.number_photons = int(photons)
+    s.num_layers = len(layers)
+    s.num_sds = len(detectors)
+    s.upper_n, s.lower_n = upper_n, lower_n
+    s.detector_reflectance = detector_reflectance
+    s.source_probe_oblique = int(bool(source_oblique))
+    s.detector_probe_oblique = int(bool(detector_oblique))
+    s.source_NA, s.source_radius, s.source_angle_deg = source
+    for i, (h, mua, mus, n, g) in enumerate(layers):
+        s.height[i], s.mua[i], s.mus[i], s.n[i], s.g[i] = h, mua, mus, n, g
+    for i, (pos, na, r, ang) in enumerate(detectors):
+        s.det_pos[i], s.det_NA[i], s.det_radius[i], s.det_angle_deg[i] = pos, na, r, ang
+    return s
+
+
+def uniform_stream(seed: int, subsequence: int, count: int, device: int = 0) -> np.ndarray:
+    """The first `count` curand_uniform draws of XORWOW subsequence
+    `subsequence` under `seed` (the stream of the reference's thread)."""
+    lib = load_library()
+    out = np.empty(count, dtype=np.float32)
+    _check(lib.mcml_uniform_stream(device, seed, subsequence, count,
+                                   out.ctypes.data_as(C.c_void_p)), "mcml_uniform_stream")
+    return out
+
+
+class Simulation:
+    """One simulation context (mcml_ctx): first pass, replay, outputs."""
+
+    def __init__(self, sim: Sim, *, seed: int = 0, slots: int = 0, device: int = 0,
+                 grid: Optional[tuple] = None, record_capacity: int = 0,
+                 stream: Optional[int] = None, block_size: int = 0, blocks_per_sm: int = 0,
+                 replay_step_budget: int = 0, slot_begin: int = 0):
+        self._lib = load_library()
+        self.sim = sim
+        o = Opts()
+        o.seed = seed
+        o.slots = slots
+        o.device = device
+        if grid is not None:
+            o.grid_nr, o.grid_nz, o.grid_dr, o.grid_dz = grid
+        o.record_capacity = record_capacity
+        o.stream = stream
+        o.block_size = block_size
+        o.blocks_per_sm = blocks_per_sm
+        o.replay_step_budget = replay_step_budget
+        o.slot_begin = slot_begin
+        self.opts = o
+        self._ctx = C.c_void_p()
+        _check(self._lib.mcml_create(C.byref(sim), C.byref(o), C.byref(self._ctx)),
+               "mcml_create")
+
+    @property
+    def num_layers(self) -> int:
+        return int(self.sim.num_layers)
+
+    @property
+    def num_sds(self) -> int:
+        return int(self.sim.num_sds)
+
+    @property
+    def grid(self) -> tuple:
+        o = self.opts
+        return (o.grid_nr or 1000, o.grid_nz or 500, o.grid_dr or 0.01, o.grid_dz or 0.01)
+
+    def set_sim(self, sim: Sim) -> None:
+        _check(self._lib.mcml_set_sim(self._ctx, C.byref(sim)), "mcml_set_sim")
+        self.sim = sim
+
+    def run(self) -> Result:
+        r = Result()
+        _check(self._lib.mcml_run(self._ctx, C.byref(r)), "mcml_run")
+        return r
+
+    def launch_run(self) -> None:
+        _check(self._lib.mcml_launch_run(self._ctx), "mcml_launch_run")
+
+    def launch_replay(self) -> None:
+        _check(self._lib.mcml_launch_replay(self._ctx), "mcml_launch_replay")
+
+    def result(self) -> Result:
+        r = Result()
+        _check(self._lib.mcml_get_result(self._ctx, C.byref(r)), "mcml_get_result")
+        return r
+
+    def replay(self) -> Result:
+        r = Result()
+        _check(self._lib.mcml_replay(self._ctx, C.byref(r)), "mcml_replay")
+        return r
+
+    def detections(self, sds: int) -> tuple[np.ndarray, np.ndarray]:
+        n = C.c_uint64(0)
+        _check(self._lib.mcml_get_detections(self._ctx, sds, None, None, 0, C.byref(n)),
+               "mcml_get_detections")
+        ids = np.empty(n.value, dtype=np.uint64)
+        w = np.empty(n.value, dtype=np.float32)
+        _check(self._lib.mcml_get_detections(self._ctx, sds, ids.ctypes.data_as(C.c_void_p),
+                                             w.ctypes.data_as(C.c_void_p), n.value,
+                                             C.byref(n)), "mcml_get_detections")
+        return ids, w
+
+    def rows(self, sds: int) -> tuple[np.ndarray, np.ndarray]:
+        L = self.num_layers
+        n = C.c_uint64(0)
+        _check(self._lib.mcml_get_rows(self._ctx, sds, None, None, 0, C.byref(n)),
+               "mcml_get_rows")
+        rows = np.empty((n.value, L + 2), dtype=np.float32)
+        inter = np.empty((n.value, L), dtype=np.uint32)
+        _check(self._lib.mcml_get_rows(self._ctx, sds, rows.ctypes.data_as(C.c_void_p),
+                                       inter.ctypes.data_as(C.c_void_p), n.value, C.byref(n)),
+               "mcml_get_rows")
+        return rows, inter
+
+    def tallies(self) -> tuple[np.ndarray, np.ndarray]:
+        nr, nz, _, _ = self.grid
+        S = self.num_sds
+        arz = np.empty((S, nz, nr), dtype=np.uint64)
+        a0z = np.empty((S, nz), dtype=np.uint64)
+        _check(self._lib.mcml_get_tallies(self._ctx, arz.ctypes.data_as(C.c_void_p),
+                                          a0z.ctypes.data_as(C.c_void_p)), "mcml_get_tallies")
+        return arz, a0z
+
+    def average_pathlength(self) -> np.ndarray:
+        out = np.empty(self.num_sds * self.num_layers, dtype=np.float64)
+        _check(self._lib.mcml_average_pathlength(self._ctx, out.ctypes.data_as(C.c_void_p)),
+               "mcml_average_pathlength")
+        return out.reshape(self.num_sds, self.num_layers)
+
+    def write_outputs(self, directory: str, output_txt: str, flags: int, sim_s: float = 0.0,
+                      replay_s: float = 0.0) -> None:
+        _check(self._lib.mcml_write_outputs(self._ctx, directory.encode(), output_txt.encode(),
+                                            flags, sim_s, replay_s), "mcml_write_outputs")
+
+    def close(self) -> None:
+        if getattr(self, "_ctx", None) and self._ctx.value:
+            self._lib.mcml_destroy(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

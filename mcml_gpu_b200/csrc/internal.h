@@ -1,0 +1,50 @@
+// internal.h -- helpers shared by the library's host translation units.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/mcml_b200.h"
+
+namespace mcml {
+
+// Records `msg` as this thread's last error and returns `code`.
+int set_error(int code, const std::string &msg);
+void clear_error();
+
+int parse_config(const char *sim_json_path, const char *input_txt_path, mcml_sim *sims,
+                 int max_sims, int *num_sims);
+int validate_sim(const mcml_sim *s);
+int derive(const mcml_sim *s, mcml_derived *out);
+
+// Everything the file writers need, on the host, in output order.
+struct HostOutputs {
+  const mcml_sim *sim;
+  const mcml_derived *der;
+  std::string gpu_name;
+  bool replayed;
+  // per SDS (0-based): detected weights' FP64 sums and counts
+  std::vector<double> weight_sum;
+  std::vector<uint64_t> detected;
+  // replay rows per SDS, (L+2) floats each, photon order
+  std::vector<std::vector<float>> rows;
+  // tallies (u64 quanta)
+  const uint64_t *A_rz = nullptr;
+  const uint64_t *A0_z = nullptr;
+  uint32_t nr = 1000, nz = 500;
+  float dr = 0.01f, dz = 0.01f;
+};
+
+// calculate_average_pathlength (transport.cu:274-297); out has S*L entries.
+void average_pathlength(const HostOutputs &o, std::vector<double> &out);
+
+// Writers (io.cpp:11-33, 281-469).  Return MCML_OK or MCML_E_IO.
+int write_output_txt(const HostOutputs &o, const std::string &path);
+int write_summary(const HostOutputs &o, const std::string &path, double sim_s, double replay_s);
+int write_pathlength(const HostOutputs &o, const std::string &dir, bool binary);
+int write_average_pathlength(const HostOutputs &o, const std::string &path);
+int write_A_rz(const HostOutputs &o, const std::string &dir, bool binary);
+int write_A0_z(const HostOutputs &o, const std::string &dir, bool binary);
+
+}  // namespace mcml

@@ -1,0 +1,206 @@
+// writers.cpp -- the reference's output files, byte for byte.
+//
+// Names, open modes and value formatting follow io.cpp:11-33 and 281-469:
+// iostream default formatting (6 significant digits) for text, float32
+// for binary, fixed file names in the working directory except the
+// caller-named reflectance file.  The value written for reflectance and
+// absorbance is computed with the reference's expressions
+// (weight / (0xFFFFFFFF*N), and / (scale*2*PI*(r+0.5)*dr*dr*dz)).
+#include <cmath>
+#include <cstdio>
+#include <fstream>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+
+namespace mcml {
+
+namespace {
+
+constexpr float kPIf = 3.141592654f;
+
+std::string join(const std::string &dir, const std::string &name) {
+  if (dir.empty()) return name;
+  if (dir.back() == '/') return dir + name;
+  return dir + "/" + name;
+}
+
+std::string numbered(const char *prefix, int sds1, const char *postfix) {
+  return std::string(prefix) + std::to_string(sds1) + postfix;
+}
+
+}  // namespace
+
+// transport.cu:274-297
+void average_pathlength(const HostOutputs &o, std::vector<double> &out) {
+  const int S = (int)o.sim->num_sds;
+  const int L = (int)o.sim->num_layers;
+  out.assign((size_t)S * L, 0.0);
+  const double inverse_start_weight = double(1 / o.der->start_weight);
+  for (int s = 0; s < S; s++) {
+    const std::vector<float> &rows = o.rows[s];
+    const size_t n = rows.size() / (size_t)(L + 2);
+    for (int l = 1; l <= L; l++) {
+      double sum_photon_reflectance = 0;
+      double sum_photon_change_reflectance = 0;
+      const double changed_mua = 0.001 * o.sim->mua[l - 1];
+      for (size_t i = 0; i < n; i++) {
+        const float *row = &rows[i * (L + 2)];
+        double photon_energy = row[0] * inverse_start_weight;
+        sum_photon_reflectance += photon_energy;
+        photon_energy *= std::exp(-1 * changed_mua * row[l]);
+        sum_photon_change_reflectance += photon_energy;
+      }
+      out[(size_t)s * L + l - 1] =
+          std::log(sum_photon_reflectance / sum_photon_change_reflectance) / changed_mua;
+    }
+  }
+}
+
+// io.cpp:11-33
+int write_output_txt(const HostOutputs &o, const std::string &path) {
+  std::ofstream f(path, std::ios::app);
+  if (!f) return set_error(MCML_E_IO, "cannot open " + path);
+  const double scale1 = (double)0xFFFFFFFF * (double)o.sim->number_photons;
+  for (unsigned i = 0; i < o.sim->num_sds; i++) f << double(o.weight_sum[i] / scale1) << " ";
+  f << std::endl;
+  return f ? MCML_OK : set_error(MCML_E_IO, "write failed: " + path);
+}
+
+// io.cpp:345-381
+int write_summary(const HostOutputs &o, const std::string &path, double sim_s, double replay_s) {
+  std::ofstream f(path, std::ios::app);
+  if (!f) return set_error(MCML_E_IO, "cannot open " + path);
+  const double N = (double)o.sim->number_photons;
+  const double scale1 = (double)0xFFFFFFFF * N;
+  f << "{\n";
+  f << "\"MCML_version_K\": " << "3.02" << ",\n";
+  f << "\"num_photon\": " << o.sim->number_photons << ",\n";
+  f << "\"sim_time\": " << sim_s << ",\n";
+  double sim_speed;
+  if (o.replayed) {
+    f << "\"replay_time\": " << replay_s << ",\n";
+    sim_speed = N / (sim_s + replay_s);
+  } else {
+    sim_speed = N / sim_s;
+  }
+  f << "\"sim_speed(photons/s)\": " << sim_speed << ",\n";
+  f << "\"sim_GPU\": \"" << o.gpu_name << "\",\n";
+  f << "\"each_photon_weight\": " << scale1 << ",\n";
+  f << "\"number_layers\": " << o.sim->num_layers << ",\n";
+  f << "\"detect_mode\": ";
+  f << (o.sim->source_probe_oblique ? "\"fiber\"" : "\"ring\"");
+  f << ",\n";
+  f << "\"num_SDS\": " << o.sim->num_sds << ",\n";
+  f << "\"SDS_detected_number\": [";
+  const unsigned S = o.sim->num_sds;
+  for (unsigned d = 0; d + 1 < S; d++) f << " " << o.detected[d] << " ,";
+  f << " " << o.detected[S - 1] << " ]\n";
+  f << "}";
+  return f ? MCML_OK : set_error(MCML_E_IO, "write failed: " + path);
+}
+
+// io.cpp:281-329
+int write_pathlength(const HostOutputs &o, const std::string &dir, bool binary) {
+  const int L = (int)o.sim->num_layers;
+  for (unsigned s = 0; s < o.sim->num_sds; s++) {
+    const std::vector<float> &rows = o.rows[s];
+    if (binary) {
+      const std::string name = join(dir, numbered("pathlength_SDS_", s + 1, ".bin"));
+      FILE *fp = std::fopen(name.c_str(), "wb");
+      if (!fp) return set_error(MCML_E_IO, "cannot open " + name);
+      const size_t n = rows.size();
+      const bool ok = n == 0 || std::fwrite(rows.data(), sizeof(float), n, fp) == n;
+      std::fclose(fp);
+      if (!ok) return set_error(MCML_E_IO, "write failed: " + name);
+    } else {
+      const std::string name = join(dir, numbered("pathlength_SDS_", s + 1, ".txt"));
+      std::ofstream f(name, std::ios::app);
+      if (!f) return set_error(MCML_E_IO, "cannot open " + name);
+      const size_t n = rows.size() / (size_t)(L + 2);
+      for (size_t i = 0; i < n; i++) {
+        for (int j = 0; j <= L + 1; j++) f << rows[i * (L + 2) + j] << '\t';
+        f << std::endl;
+      }
+      if (!f) return set_error(MCML_E_IO, "write failed: " + name);
+    }
+  }
+  return MCML_OK;
+}
+
+// io.cpp:331-343
+int write_average_pathlength(const HostOutputs &o, const std::string &path) {
+  std::vector<double> avg;
+  average_pathlength(o, avg);
+  std::ofstream f(path, std::ios::app);
+  if (!f) return set_error(MCML_E_IO, "cannot open " + path);
+  const unsigned L = o.sim->num_layers;
+  for (unsigned s = 0; s < o.sim->num_sds; s++)
+    for (unsigned l = 0; l < L; l++) f << avg[(size_t)s * L + l] << '\t';
+  f << std::endl;
+  return f ? MCML_OK : set_error(MCML_E_IO, "write failed: " + path);
+}
+
+// io.cpp:383-434
+int write_A_rz(const HostOutputs &o, const std::string &dir, bool binary) {
+  const double scale1 = (double)0xFFFFFFFF * (double)o.sim->number_photons;
+  const uint32_t nr = o.nr, nz = o.nz;
+  const float dr = o.dr, dz = o.dz;
+  std::vector<double> scale2(nr);
+  for (uint32_t r = 0; r < nr; r++) scale2[r] = scale1 * 2 * kPIf * (r + 0.5) * dr * dr * dz;
+  for (unsigned s = 0; s < o.sim->num_sds; s++) {
+    const uint64_t *data = o.A_rz + (size_t)s * nr * nz;
+    if (binary) {
+      const std::string name = join(dir, numbered("A_rz_SDS_", s + 1, ".bin"));
+      FILE *fp = std::fopen(name.c_str(), "wb");
+      if (!fp) return set_error(MCML_E_IO, "cannot open " + name);
+      std::vector<float> buf((size_t)nr * nz);
+      for (uint32_t z = 0; z < nz; z++)
+        for (uint32_t r = 0; r < nr; r++)
+          buf[(size_t)z * nr + r] = float(double(data[(size_t)z * nr + r] / scale2[r]));
+      const bool ok = std::fwrite(buf.data(), sizeof(float), buf.size(), fp) == buf.size();
+      std::fclose(fp);
+      if (!ok) return set_error(MCML_E_IO, "write failed: " + name);
+    } else {
+      const std::string name = join(dir, numbered("A_rz_SDS_", s + 1, ".txt"));
+      std::ofstream f(name, std::ios::app);
+      if (!f) return set_error(MCML_E_IO, "cannot open " + name);
+      for (uint32_t z = 0; z < nz; z++) {
+        for (uint32_t r = 0; r < nr; r++) f << double(data[(size_t)z * nr + r] / scale2[r]) << "\t";
+        f << std::endl;
+      }
+      if (!f) return set_error(MCML_E_IO, "write failed: " + name);
+    }
+  }
+  return MCML_OK;
+}
+
+// io.cpp:436-469
+int write_A0_z(const HostOutputs &o, const std::string &dir, bool binary) {
+  const double scale1 = (double)0xFFFFFFFF * (double)o.sim->number_photons;
+  const double scale2 = scale1 * 2 * kPIf * (0 + 0.5) * o.dr * o.dr * o.dz;
+  const uint32_t nz = o.nz;
+  for (unsigned s = 0; s < o.sim->num_sds; s++) {
+    const uint64_t *data = o.A0_z + (size_t)s * nz;
+    if (binary) {
+      const std::string name = join(dir, numbered("A0_z_SDS_", s + 1, ".bin"));
+      FILE *fp = std::fopen(name.c_str(), "wb");
+      if (!fp) return set_error(MCML_E_IO, "cannot open " + name);
+      std::vector<float> buf(nz);
+      for (uint32_t z = 0; z < nz; z++) buf[z] = float(double(data[z] / scale2));
+      const bool ok = std::fwrite(buf.data(), sizeof(float), nz, fp) == nz;
+      std::fclose(fp);
+      if (!ok) return set_error(MCML_E_IO, "write failed: " + name);
+    } else {
+      const std::string name = join(dir, numbered("A0_z_SDS_", s + 1, ".txt"));
+      std::ofstream f(name, std::ios::app);
+      if (!f) return set_error(MCML_E_IO, "cannot open " + name);
+      for (uint32_t z = 0; z < nz; z++) f << double(data[z] / scale2) << std::endl;
+      if (!f) return set_error(MCML_E_IO, "write failed: " + name);
+    }
+  }
+  return MCML_OK;
+}
+
+}  // namespace mcml
