@@ -206,7 +206,10 @@ def mcml_arm(args) -> int:
     N = int(sim.number_photons)
     info = m.device_info(local)
     slots = args.slots or int(info.reference_threads)
-    stream = torch.cuda.current_stream()
+    # A dedicated (non-default) stream: the library launches on it and the
+    # CUDA events below are recorded on it.
+    stream = torch.cuda.Stream(device=local)
+    torch.cuda.set_stream(stream)
     run = m.Simulation(sim, seed=args.seed + rank, slots=slots, slot_begin=rank * slots,
                        device=local, stream=stream.cuda_stream, block_size=args.block,
                        blocks_per_sm=args.blocks_per_sm)

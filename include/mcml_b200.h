@@ -84,11 +84,13 @@ typedef struct mcml_sim {
 /* Run options.  Zero-initialise and set what you need. */
 typedef struct mcml_opts {
   uint64_t seed;            /* XORWOW seed (reference: time(NULL), transport.cu:72) */
-  uint64_t slots;           /* RNG subsequences ("photon slots"); 0 = the reference's
-                               thread count on this device, SMs x max threads/SM
-                               (io.cpp:522-526), so that slot t walks the photons the
-                               reference's thread t walks.  N==slots gives the
-                               reference's one-photon-per-thread layout.            */
+  uint64_t slots;           /* RNG subsequences ("photon slots"): slot s walks its
+                               photons in order on subsequence s, as the reference's
+                               thread s does.  0 = automatic: N when N is at most
+                               the reference's thread count on this device
+                               (SMs x max threads/SM, io.cpp:522-526) -- its
+                               one-photon-per-thread layout, bit-exact when N equals
+                               it -- else about 8 photons per slot.                  */
   int32_t device;           /* CUDA ordinal (reference: -G, main.cu:51-59)          */
   uint32_t grid_nr;         /* absorbance grid; 0 = 1000                            */
   uint32_t grid_nz;         /* 0 = 500                                              */

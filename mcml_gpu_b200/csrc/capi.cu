@@ -63,6 +63,11 @@ void dfree(T *&p) {
 }
 
 constexpr uint64_t kDefaultBudget = 1ull << 26;
+// Automatic slot count for N above the reference's thread count: about
+// this many photons per slot keeps the end-of-launch tail (one slot of
+// work) small against each lane's share, at one skipahead per slot.
+constexpr uint64_t kPhotonsPerSlot = 8;
+constexpr uint64_t kMaxAutoSlots = 1ull << 26;
 
 }  // namespace
 
@@ -94,6 +99,7 @@ struct mcml_ctx {
   // [0] first pass start, [4] walk start, [1] walk end, [2]/[3] replay
   cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   int walk_block = 128;
+  int walk_min_blocks = 8;
   int walk_grid = 0;
   int replay_grid = 0;
   bool ran = false, replayed = false;
@@ -178,10 +184,20 @@ int set_sim(mcml_ctx *c, const mcml_sim *sim) {
   c->sim = *sim;
   c->N = sim->number_photons;
   const uint64_t ref_threads = (uint64_t)c->sm_count * (uint64_t)c->max_thr_sm;
-  uint64_t S = c->opts.slots ? c->opts.slots : ref_threads;
+  uint64_t S;
+  if (c->opts.slots) {
+    S = c->opts.slots;
+  } else if (c->N <= ref_threads) {
+    S = c->N;  // the reference's layout: photon t is thread t's first photon
+  } else {
+    S = (c->N + kPhotonsPerSlot - 1) / kPhotonsPerSlot;
+    S = std::max(S, ref_threads);
+    S = std::min(S, std::max(kMaxAutoSlots, ref_threads));
+  }
   if (S > c->N) S = c->N;
   if (c->N / S >= 0xFFFFFFFFull)
     return set_error(MCML_E_INVALID, "too many photons per slot; raise mcml_opts.slots");
+  if (S >= 0xFFFFFFFFull) return set_error(MCML_E_INVALID, "slots must be below 2^32");
   c->S = S;
   const uint64_t nz = grid_nz(c), nr = grid_nr(c);
   if (nr == 0 || nz == 0 || (uint64_t)sim->num_sds * nz * nr >= (1ull << 31))
@@ -302,8 +318,8 @@ int launch_run(mcml_ctx *c) {
   A.records = c->d_records;
   A.rec_cap = c->rec_cap;
   CUDA_TRY(launch_walk(c->P, A, c->sim.source_probe_oblique != 0,
-                       c->sim.detector_probe_oblique != 0, c->walk_block, c->walk_grid,
-                       c->stream));
+                       c->sim.detector_probe_oblique != 0, c->walk_block, c->walk_min_blocks,
+                       c->walk_grid, c->stream));
   CUDA_TRY(cudaEventRecord(c->ev[1], c->stream));
   CUDA_TRY(launch_reduce_records(c->d_records, c->d_counters + kCntRecords, c->rec_cap,
                                  c->sim.num_sds, c->d_sums,
@@ -365,6 +381,32 @@ int launch_replay(mcml_ctx *c) {
   CUDA_TRY(cudaEventRecord(c->ev[3], c->stream));
   c->replayed = true;
   c->host_valid = false;
+  return MCML_OK;
+}
+
+// Walk launch shape: threads per block and the register-capping minimum
+// of resident blocks per SM; the grid fills every SM with as many blocks
+// as fit.  Defaults: 128 threads, 8 blocks (64 registers per thread).
+int choose_walk(mcml_ctx *c) {
+  const int block = c->opts.block_size ? (int)c->opts.block_size : 128;
+  int minb = c->opts.blocks_per_sm ? (int)c->opts.blocks_per_sm : (block == 128 ? 8 : 2048 / block / 2);
+  const bool so = c->sim.source_probe_oblique != 0, dobl = c->sim.detector_probe_oblique != 0;
+  const void *fn = walk_kernel_ptr(block, minb, so, dobl);
+  bool limit = false;  // no variant capped for minb: run the uncapped one, minb blocks/SM
+  if (!fn) {
+    limit = c->opts.blocks_per_sm != 0;
+    minb = 1;
+    fn = walk_kernel_ptr(block, 1, so, dobl);
+  }
+  if (!fn) return set_error(MCML_E_INVALID, "block_size must be 64, 128 or 256");
+  DeviceGuard g(c->device);
+  int nb = 0;
+  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, block, 0));
+  if (limit && (int)c->opts.blocks_per_sm < nb) nb = (int)c->opts.blocks_per_sm;
+  if (nb < 1) nb = 1;
+  c->walk_block = block;
+  c->walk_min_blocks = minb;
+  c->walk_grid = nb * c->sm_count;
   return MCML_OK;
 }
 
@@ -504,15 +546,8 @@ int mcml_create(const mcml_sim *sim, const mcml_opts *opts, mcml_ctx **out) {
   }
   rc = ensure_records(c.get(), cap);
   if (rc) return rc;
-  c->walk_block = o.block_size ? (int)o.block_size : 128;
-  const void *fn = walk_kernel_ptr(c->walk_block, sim->source_probe_oblique != 0,
-                                   sim->detector_probe_oblique != 0);
-  if (!fn) return set_error(MCML_E_INVALID, "block_size must be 64, 128 or 256");
-  int nb = 0;
-  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, c->walk_block, 0));
-  if (o.blocks_per_sm) nb = (int)o.blocks_per_sm;
-  if (nb < 1) nb = 1;
-  c->walk_grid = nb * c->sm_count;
+  rc = choose_walk(c.get());
+  if (rc) return rc;
   c->replay_grid = 8 * c->sm_count;
   *out = c.release();
   return MCML_OK;
@@ -523,19 +558,11 @@ int mcml_set_sim(mcml_ctx *ctx, const mcml_sim *sim) {
   if (!ctx) return set_error(MCML_E_INVALID, "null context");
   const int rc = validate_sim(sim);
   if (rc) return rc;
-  if (sim->source_probe_oblique != ctx->sim.source_probe_oblique ||
-      sim->detector_probe_oblique != ctx->sim.detector_probe_oblique) {
-    // launch shape was sized for the kernel variant; recompute it
-    const void *fn = walk_kernel_ptr(ctx->walk_block, sim->source_probe_oblique != 0,
-                                     sim->detector_probe_oblique != 0);
-    int nb = 0;
-    DeviceGuard g(ctx->device);
-    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, ctx->walk_block, 0));
-    if (ctx->opts.blocks_per_sm) nb = (int)ctx->opts.blocks_per_sm;
-    ctx->walk_grid = std::max(nb, 1) * ctx->sm_count;
-  }
-  return set_sim(ctx, sim);
+  int rc2 = set_sim(ctx, sim);
+  if (rc2) return rc2;
+  return choose_walk(ctx);
 }
+
 
 void mcml_destroy(mcml_ctx *ctx) { delete ctx; }
 

@@ -61,32 +61,38 @@ __device__ __forceinline__ void clear_gauss(curandStateXORWOW &st) {
   st.boxmuller_extra_double = 0.0;
 }
 
-struct SeedCopy {
-  uint32_t d, v0, v1, v2, v3, v4;
+// The XORWOW state at the launch of each lane's current photon, kept in
+// shared memory (written once per photon, read only on a detection).
+template <int kBlock>
+struct SeedStore {
+  uint32_t w[6][kBlock];
   __device__ __forceinline__ void save(const curandStateXORWOW &st) {
-    d = st.d;
-    v0 = st.v[0];
-    v1 = st.v[1];
-    v2 = st.v[2];
-    v3 = st.v[3];
-    v4 = st.v[4];
+    const int t = threadIdx.x;
+    w[0][t] = st.d;
+    w[1][t] = st.v[0];
+    w[2][t] = st.v[1];
+    w[3][t] = st.v[2];
+    w[4][t] = st.v[3];
+    w[5][t] = st.v[4];
   }
 };
 
+template <int kBlock>
 __device__ __forceinline__ void append_record(const WalkArgs &A, uint64_t photon, int sds,
-                                              float w, const SeedCopy &sc) {
+                                              float w, const SeedStore<kBlock> &sc) {
   const unsigned long long idx = atomicAdd(&A.counters[kCntRecords], 1ull);
   if (idx < A.rec_cap) {
+    const int t = threadIdx.x;
     DetRecord r;
     r.photon = photon;
     r.sds = (uint32_t)sds;
     r.weight = w;
-    r.d = sc.d;
-    r.v[0] = sc.v0;
-    r.v[1] = sc.v1;
-    r.v[2] = sc.v2;
-    r.v[3] = sc.v3;
-    r.v[4] = sc.v4;
+    r.d = sc.w[0][t];
+    r.v[0] = sc.w[1][t];
+    r.v[1] = sc.w[2][t];
+    r.v[2] = sc.w[3][t];
+    r.v[3] = sc.w[4][t];
+    r.v[4] = sc.w[5][t];
     A.records[idx] = r;
   }
 }
@@ -95,25 +101,33 @@ __device__ __forceinline__ void append_record(const WalkArgs &A, uint64_t photon
 
 // ---------------------------------------------------------------------------
 // Slot seeding: state of subsequence s at offset 0 (LaunchPhoton_Global's
-// curand_init, transport.cu:733), 24 bytes per slot.
+// curand_init, transport.cu:733), 24 bytes per slot.  Each thread seeds a
+// run of consecutive slots: curand_init for the first, then
+// skipahead_sequence(1) -- one precomputed-matrix step of 2^67 draws --
+// for each next one, which is far cheaper than a full curand_init.
 __global__ void seed_slots_kernel(uint64_t seed, uint64_t slot_begin, uint64_t num_slots,
-                                  uint2 *out) {
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; s < num_slots; s += stride) {
-    curandStateXORWOW st;
-    curand_init(seed, slot_begin + s, 0, &st);
+                                  uint64_t run, uint2 *out) {
+  const uint64_t s0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * run;
+  if (s0 >= num_slots) return;
+  const uint64_t s1 = s0 + run < num_slots ? s0 + run : num_slots;
+  curandStateXORWOW st;
+  curand_init(seed, slot_begin + s0, 0, &st);
+  for (uint64_t s = s0;;) {
     out[s * 3 + 0] = make_uint2(st.d, st.v[0]);
     out[s * 3 + 1] = make_uint2(st.v[1], st.v[2]);
     out[s * 3 + 2] = make_uint2(st.v[3], st.v[4]);
+    if (++s >= s1) break;
+    skipahead_sequence(1ull, &st);
   }
 }
 
 // ---------------------------------------------------------------------------
 // First pass (MCd, transport.cu:341-471).
-template <int kBlock, bool kSrcOblique, bool kDetOblique>
-__global__ void __launch_bounds__(kBlock) walk_kernel(const __grid_constant__ DevParams P,
-                                                      const WalkArgs A) {
+template <int kBlock, int kMinBlocks, bool kSrcOblique, bool kDetOblique>
+__global__ void __launch_bounds__(kBlock, kMinBlocks)
+    walk_kernel(const __grid_constant__ DevParams P, const WalkArgs A) {
   __shared__ SmemTables t;
+  __shared__ SeedStore<kBlock> sc;
   load_tables(t, P);
   __syncthreads();
 
@@ -127,19 +141,24 @@ __global__ void __launch_bounds__(kBlock) walk_kernel(const __grid_constant__ De
 
   curandStateXORWOW st;
   clear_gauss(st);
-  SeedCopy sc;
   Photon p;
-  uint64_t photon = 0;
-  uint64_t left = 0;
+  uint32_t slot = 0;   // current slot (S < 2^32)
+  uint32_t k = 0;      // ordinal of the current photon within its slot
+  uint32_t quota = 0;  // photons of the current slot
   uint32_t steps_acc = 0;
 
   auto next_slot = [&]() -> bool {
-    const uint64_t slot = fetch_one(&A.counters[kCntSlot]);
-    if (slot >= S) return false;
-    load_state(st, A.slot_state, slot);
-    photon = slot * q + (slot < rem ? slot : rem);
-    left = q + (slot < rem ? 1 : 0) - 1;
+    const uint64_t s = fetch_one(&A.counters[kCntSlot]);
+    if (s >= S) return false;
+    slot = (uint32_t)s;
+    load_state(st, A.slot_state, s);
+    k = 0;
+    quota = (uint32_t)(q + (s < rem ? 1 : 0));
     return true;
+  };
+  auto photon_index = [&]() -> uint64_t {
+    const uint64_t s = slot;
+    return s * q + (s < rem ? s : rem) + k;
   };
 
   if (!next_slot()) return;
@@ -150,7 +169,6 @@ __global__ void __launch_bounds__(kBlock) walk_kernel(const __grid_constant__ De
     float s;
     const int new_layer = hop(p, s, &st, t);
     p.steps++;
-    ++steps_acc;
     clamp_z(p, t, p.layer);
 
     if (new_layer != p.layer) {
@@ -160,19 +178,20 @@ __global__ void __launch_bounds__(kBlock) walk_kernel(const __grid_constant__ De
         if (new_layer == 0) {
           bool detected = false;
           if (kDetOblique) {
-            for (int i = 1; i <= n_sds; i++) {
-              if (fiber_hit(p, t, i)) {
-                append_record(A, photon, i, p.w, sc);
-                detected = true;
-              }
+            unsigned mask = fiber_mask(p, t, n_sds);
+            detected = mask != 0u;
+            while (mask) {
+              const int i = __ffs(mask) - 1;
+              mask &= mask - 1u;
+              append_record(A, photon_index(), i, p.w, sc);
             }
           } else {
             const float uz_angle = acosf(fabsf(p.dz));
-            const float distance = sqrtf(p.x * p.x + p.y * p.y);
+            const float distance = radius_xy(p);
             for (int i = 1; i <= n_sds; i++) {
               float wd;
               if (ring_hit(p, t, i, uz_angle, distance, wd)) {
-                append_record(A, photon, i, wd, sc);
+                append_record(A, photon_index(), i, wd, sc);
                 detected = true;
               }
             }
@@ -198,18 +217,12 @@ __global__ void __launch_bounds__(kBlock) walk_kernel(const __grid_constant__ De
     }
 
     if (!survive<true>(p, &st)) {
-      if (left > 0) {
-        --left;
-        ++photon;
-      } else {
-        atomicAdd(&A.counters[kCntSteps], (unsigned long long)steps_acc);
-        steps_acc = 0;
-        if (!next_slot()) break;
-      }
-      if (steps_acc >= 0x40000000u) {
+      steps_acc += (uint32_t)p.steps;  // steps of the photon that just ended
+      if (++k >= quota || steps_acc >= 0x40000000u) {
         atomicAdd(&A.counters[kCntSteps], (unsigned long long)steps_acc);
         steps_acc = 0;
       }
+      if (k >= quota && !next_slot()) break;
       sc.save(st);
       launch_photon<kSrcOblique>(p, &st, t, start_w);
     }
@@ -288,7 +301,7 @@ __global__ void __launch_bounds__(kBlock) replay_kernel(const __grid_constant__ 
               wd = p.w;
             } else {
               const float uz_angle = acosf(fabsf(p.dz));
-              const float distance = sqrtf(p.x * p.x + p.y * p.y);
+              const float distance = radius_xy(p);
               hit = ring_hit(p, t, sds, uz_angle, distance, wd);
             }
             if (hit) {
@@ -327,9 +340,9 @@ __global__ void __launch_bounds__(kBlock) replay_kernel(const __grid_constant__ 
         } else {
           int ir;
           if (kRefGrid)
-            ir = min(__float2int_rz(__fdividef(sqrtf(p.x * p.x + p.y * p.y), 0.01f)), (int)1000 - 1);
+            ir = min(__float2int_rz(__fdividef(radius_xy(p), 0.01f)), (int)1000 - 1);
           else
-            ir = min(__float2int_rz(__fdividef(sqrtf(p.x * p.x + p.y * p.y), dr)), nr - 1);
+            ir = min(__float2int_rz(__fdividef(radius_xy(p), dr)), nr - 1);
           const unsigned index = sds0 * nr * nz + iz * nr + ir;
           if (index == index_old) {
             w_run += w_temp;
@@ -410,52 +423,56 @@ cudaError_t launch_seed_slots(uint64_t seed, uint64_t slot_begin, uint64_t num_s
                               int sm_count, cudaStream_t stream) {
   if (num_slots == 0) return cudaSuccess;
   const int block = 256;
-  uint64_t want = (num_slots + block - 1) / block;
-  const uint64_t cap = (uint64_t)sm_count * 16;
-  const int grid = (int)(want < cap ? want : cap);
-  seed_slots_kernel<<<grid, block, 0, stream>>>(seed, slot_begin, num_slots, out);
+  const uint64_t threads = (uint64_t)sm_count * 2048;  // one resident wave
+  const uint64_t run = (num_slots + threads - 1) / threads;
+  const uint64_t used = (num_slots + run - 1) / run;
+  const int grid = (int)((used + block - 1) / block);
+  seed_slots_kernel<<<grid, block, 0, stream>>>(seed, slot_begin, num_slots, run, out);
   return cudaGetLastError();
 }
 
-template <int kBlock>
-static cudaError_t walk_dispatch(const DevParams &P, const WalkArgs &A, bool src_obl,
-                                 bool det_obl, int grid, cudaStream_t stream) {
-  if (src_obl && det_obl)
-    walk_kernel<kBlock, true, true><<<grid, kBlock, 0, stream>>>(P, A);
-  else if (src_obl)
-    walk_kernel<kBlock, true, false><<<grid, kBlock, 0, stream>>>(P, A);
-  else if (det_obl)
-    walk_kernel<kBlock, false, true><<<grid, kBlock, 0, stream>>>(P, A);
-  else
-    walk_kernel<kBlock, false, false><<<grid, kBlock, 0, stream>>>(P, A);
-  return cudaGetLastError();
+// Walk variants: (threads per block, minimum resident blocks per SM).  The
+// second number caps the registers per thread (65536 / (threads * blocks)).
+struct WalkVariant {
+  int block, min_blocks;
+  const void *fn[4];  // [src_oblique*2 + det_oblique]
+};
+
+template <int B, int M>
+static WalkVariant make_variant() {
+  return WalkVariant{B,
+                     M,
+                     {(const void *)walk_kernel<B, M, false, false>,
+                      (const void *)walk_kernel<B, M, false, true>,
+                      (const void *)walk_kernel<B, M, true, false>,
+                      (const void *)walk_kernel<B, M, true, true>}};
 }
 
-template <int kBlock>
-static const void *walk_fn(bool src_obl, bool det_obl) {
-  if (src_obl && det_obl) return (const void *)walk_kernel<kBlock, true, true>;
-  if (src_obl) return (const void *)walk_kernel<kBlock, true, false>;
-  if (det_obl) return (const void *)walk_kernel<kBlock, false, true>;
-  return (const void *)walk_kernel<kBlock, false, false>;
+static const WalkVariant *walk_variants(int *n) {
+  static const WalkVariant v[] = {
+      make_variant<64, 1>(),  make_variant<128, 1>(), make_variant<256, 1>(),
+      make_variant<128, 8>(), make_variant<128, 10>(), make_variant<128, 12>(),
+      make_variant<256, 4>(), make_variant<256, 5>(),  make_variant<256, 6>(),
+  };
+  *n = (int)(sizeof(v) / sizeof(v[0]));
+  return v;
 }
 
-const void *walk_kernel_ptr(int block, bool src_obl, bool det_obl) {
-  switch (block) {
-    case 64: return walk_fn<64>(src_obl, det_obl);
-    case 128: return walk_fn<128>(src_obl, det_obl);
-    case 256: return walk_fn<256>(src_obl, det_obl);
-    default: return nullptr;
-  }
+const void *walk_kernel_ptr(int block, int min_blocks, bool src_obl, bool det_obl) {
+  int n = 0;
+  const WalkVariant *v = walk_variants(&n);
+  for (int i = 0; i < n; ++i)
+    if (v[i].block == block && v[i].min_blocks == min_blocks)
+      return v[i].fn[(src_obl ? 2 : 0) + (det_obl ? 1 : 0)];
+  return nullptr;
 }
 
 cudaError_t launch_walk(const DevParams &P, const WalkArgs &A, bool src_obl, bool det_obl,
-                        int block, int grid, cudaStream_t stream) {
-  switch (block) {
-    case 64: return walk_dispatch<64>(P, A, src_obl, det_obl, grid, stream);
-    case 128: return walk_dispatch<128>(P, A, src_obl, det_obl, grid, stream);
-    case 256: return walk_dispatch<256>(P, A, src_obl, det_obl, grid, stream);
-    default: return cudaErrorInvalidValue;
-  }
+                        int block, int min_blocks, int grid, cudaStream_t stream) {
+  const void *fn = walk_kernel_ptr(block, min_blocks, src_obl, det_obl);
+  if (!fn) return cudaErrorInvalidValue;
+  void *args[] = {(void *)&P, (void *)&A};
+  return cudaLaunchKernel(fn, dim3(grid), dim3(block), args, 0, stream);
 }
 
 template <bool kSrc, bool kDet>

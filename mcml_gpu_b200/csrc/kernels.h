@@ -45,8 +45,8 @@ struct ReplayArgs {
 cudaError_t launch_seed_slots(uint64_t seed, uint64_t slot_begin, uint64_t num_slots, uint2 *out,
                               int sm_count, cudaStream_t stream);
 cudaError_t launch_walk(const DevParams &P, const WalkArgs &A, bool src_obl, bool det_obl,
-                        int block, int grid, cudaStream_t stream);
-const void *walk_kernel_ptr(int block, bool src_obl, bool det_obl);
+                        int block, int min_blocks, int grid, cudaStream_t stream);
+const void *walk_kernel_ptr(int block, int min_blocks, bool src_obl, bool det_obl);
 cudaError_t launch_replay(const DevParams &P, const ReplayArgs &A, bool src_obl, bool det_obl,
                           bool ref_grid, int grid, cudaStream_t stream);
 cudaError_t launch_reduce_records(const DetRecord *rec, const unsigned long long *rec_count,
