@@ -40,21 +40,26 @@ CONFIG = ROOT / "tests" / "golden" / "configs" / "c1"
 METRIC = "photons/s (plain MC)"
 WORKLOAD = "plain MC + replay, 5-layer tissue, 1e8 photons, -R -A -B (config 1)"
 
-# Per-step work of the walk, counted by hand from the step's arithmetic
-# (hop + drop + Henyey-Greenstein spin + roulette test, the path a step
-# takes when it neither crosses a boundary nor plays roulette):
-#   XORWOW draw: 9 integer ops + 1 convert + 1 FMA; 3 draws per step.
-#   FP32/INT32 lane ops per step ........................ OPS_LANE
-#   quarter-rate ops (MUFU lg2/rcp/sin/cos/rsqrt/sqrt, and
-#   int<->float conversions) per step ................... OPS_XU
-# B200 SM per clock: 128 FP32 lanes, 16 MUFU/conversion lanes.
-OPS_LANE = 118
-OPS_XU = 15
+# Per-step work of the walk, counted by hand from the step's arithmetic for
+# the common step (hop + weight drop + Henyey-Greenstein spin + roulette
+# test; no boundary, no roulette draw):
+#   3 XORWOW draws: 9 integer ops + 1 FMA each (lane), 1 int->float (XU)
+#   hop: 2 mul, 2 fma + 2 cmp (boundary), 3 fma (move), 1 add, 4 clamp,
+#        1 cmp (lane); lg2 (XU)
+#   drop: 2 mul, 1 sub (lane); 2 float->int, 2 int->float (XU)
+#   spin: HG 10, two IEEE sqrt 2x5, sincos 2, rotation 15, renormalise 6,
+#        1 cmp (lane); 2 rcp, 2 rsq (sqrt), sin, cos, 2 rcp, rsq (XU)
+#   survive: 2 cmp (lane)
+# = 94 FP32/INT32 lane ops and 17 quarter-rate (MUFU + conversion) ops.
+# A B200 SM issues 128 thread-instructions and 16 XU results per clock, so
+# steps/s <= f_sm * 148 * min(128 / (94 + 17), 16 / 17): the XU pipe binds.
+OPS_LANE = 94
+OPS_XU = 17
 SM_COUNT = 148
 
 
 def steps_per_clock_per_sm() -> float:
-    return min(128.0 / OPS_LANE, 16.0 / OPS_XU)
+    return min(128.0 / (OPS_LANE + OPS_XU), 16.0 / OPS_XU)
 
 
 class ClockSampler:
@@ -179,12 +184,58 @@ def reference_arm(args) -> int:
     return 0
 
 
-def read_traffic() -> float | None:
+def reference_gpu_arm(args) -> int:
+    """The reference's own CUDA build (oracle/_ref/MCML_GPU, compiled from its
+    sources for sm_100a) on the benchmark workload, wall-clock timed end to
+    end per run (process start to exit, its file output included).  Seeded
+    through the time() shim; N >= its thread count, as it requires."""
+    import shutil
+    import subprocess
+    import oracle
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    if not oracle.REF_BIN.exists():
+        print(json.dumps({"impl": "reference-gpu", "unavailable": "oracle/_ref not built"}))
+        return 0
+    sim_json = json.loads((CONFIG / "sim_set.json").read_text())
+    if args.photons:
+        sim_json["number_photons"] = args.photons
+    N = int(sim_json["number_photons"])
+    times = []
+    with tempfile.TemporaryDirectory() as td:
+        (Path(td) / "sim_set.json").write_text(json.dumps(sim_json))
+        shutil.copy(CONFIG / "input.txt", Path(td) / "input.txt")
+        env = dict(os.environ, MCML_FIXED_TIME="1234", LD_PRELOAD=str(oracle.REF_SHIM))
+        for k in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            res = subprocess.run([str(oracle.REF_BIN), "sim_set.json", "input.txt", "output.txt",
+                                  "-R", "-A", "-B"], cwd=td, env=env, capture_output=True,
+                                 text=True, timeout=3600)
+            dt = time.perf_counter() - t0
+            if res.returncode != 0:
+                print(json.dumps({"impl": "reference-gpu", "unavailable": f"exit {res.returncode}"}))
+                return 0
+            if k >= args.warmup:
+                times.append(dt)
+    ms = 1000 * sum(times) / len(times)
+    print(json.dumps({"metric": METRIC, "impl": "reference-gpu", "value": N / (ms / 1000),
+                      "unit": "photons/s", "ms_per_step": ms, "steps": args.steps,
+                      "warmup": args.warmup, "photons": N,
+                      "note": "reference CUDA build, wall clock per run incl. output files"}),
+          flush=True)
+    return 0
+
+
+def read_traffic(slots: int) -> float | None:
+    """DRAM bytes of one walk launch: the ncu-measured bytes per slot of a
+    smaller capture (profiles/walk_kernel_traffic.json) times this run's
+    slot count -- the walk's DRAM traffic is the slot-state reads."""
     p = ROOT / "profiles" / "walk_kernel_traffic.json"
     if not p.exists():
         return None
     try:
-        return float(json.loads(p.read_text())["dram_bytes_per_launch"])
+        return float(json.loads(p.read_text())["dram_bytes_per_slot"]) * slots
     except Exception:
         return None
 
@@ -205,12 +256,14 @@ def mcml_arm(args) -> int:
     sim = load_sim(args.photons)
     N = int(sim.number_photons)
     info = m.device_info(local)
-    slots = args.slots or int(info.reference_threads)
+    slots = args.slots  # 0: the library's automatic slot count
     # A dedicated (non-default) stream: the library launches on it and the
     # CUDA events below are recorded on it.
     stream = torch.cuda.Stream(device=local)
     torch.cuda.set_stream(stream)
-    run = m.Simulation(sim, seed=args.seed + rank, slots=slots, slot_begin=rank * slots,
+    # Each rank walks its own range of RNG subsequences (weak scaling).
+    first, _ = m.shard(rank, world, slots or N, weak=True)
+    run = m.Simulation(sim, seed=args.seed, slots=slots, slot_begin=first,
                        device=local, stream=stream.cuda_stream, block_size=args.block,
                        blocks_per_sm=args.blocks_per_sm)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
@@ -293,7 +346,7 @@ def mcml_arm(args) -> int:
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
         "config": {"workload": WORKLOAD, "photons": N, "layers": L, "sds": S,
-                   "grid": "1000x500 @ 0.01 cm", "slots": slots,
+                   "grid": "1000x500 @ 0.01 cm", "slots": int(res.slots),
                    "l2": "flushed between steps (256 MiB write)",
                    "parallelism": f"replicas x{world}, disjoint RNG subsequences",
                    "steps_per_photon": round(steps_per_photon, 2),
@@ -304,10 +357,11 @@ def mcml_arm(args) -> int:
         "gpu_launches": 4 * args.steps,
         "roofline": {"bound": "issue", "achieved": achieved / 1e9, "peak": peak / 1e9,
                      "unit": "Gstep/s", "frac": achieved / peak,
-                     "traffic": read_traffic(),
+                     "traffic": read_traffic(int(res.slots)),
                      "kernel": "walk_kernel",
-                     "model": f"steps/s <= f_sm x {info.sm_count} SMs x min(128/{OPS_LANE}, "
-                              f"16/{OPS_XU}) at the measured median SM clock",
+                     "model": f"steps/s <= f_sm x {info.sm_count} SMs x min(128/({OPS_LANE}+"
+                              f"{OPS_XU}), 16/{OPS_XU}) at the measured median SM clock "
+                              f"(XU-pipe bound); ops counted by hand per common step",
                      "walk_ms": walk_kernel_ms, "seed_ms": float(res.seed_ms),
                      "replay_ms": float(rep.replay_ms)},
         "clocks": clocks,
@@ -329,7 +383,7 @@ def main() -> int:
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", choices=["mcml", "reference"], default="mcml")
+    ap.add_argument("--impl", choices=["mcml", "reference", "reference-gpu"], default="mcml")
     ap.add_argument("--photons", type=int, default=0, help="override N (default: 1e8)")
     ap.add_argument("--slots", type=int, default=0)
     ap.add_argument("--block", type=int, default=0)
@@ -341,6 +395,8 @@ def main() -> int:
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
+    if args.impl == "reference-gpu":
+        return reference_gpu_arm(args)
     return mcml_arm(args)
 
 

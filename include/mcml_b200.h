@@ -118,6 +118,7 @@ typedef struct mcml_result {
   float walk_ms;                     /* device time of the walk kernel        */
   float replay_ms;                   /* device time of the replay             */
   float seed_ms;                     /* device time of the slot seeding       */
+  uint64_t slots;                    /* RNG subsequences the run used         */
 } mcml_result;
 
 typedef struct mcml_device_info {

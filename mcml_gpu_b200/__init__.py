@@ -101,6 +101,7 @@ class Result(C.Structure):
         ("walk_ms", C.c_float),
         ("replay_ms", C.c_float),
         ("seed_ms", C.c_float),
+        ("slots", C.c_uint64),
     ]
 
     def as_dict(self) -> dict:
@@ -115,6 +116,8 @@ class Result(C.Structure):
             "std_error": list(self.std_error[:s]),
             "walk_ms": float(self.walk_ms),
             "replay_ms": float(self.replay_ms),
+            "seed_ms": float(self.seed_ms),
+            "slots": int(self.slots),
         }
 
 
@@ -256,6 +259,22 @@ def make_sim(layers: Sequence[Sequence[float]], detectors: Sequence[Sequence[flo
     for i, (pos, na, r, ang) in enumerate(detectors):
         s.det_pos[i], s.det_NA[i], s.det_radius[i], s.det_angle_deg[i] = pos, na, r, ang
     return s
+
+
+def shard(rank: int, world: int, photons: int, weak: bool = True) -> tuple[int, int]:
+    """(first subsequence, photon count) of one rank of a multi-GPU run.
+
+    Photons are independent, so ranks walk disjoint ranges of XORWOW
+    subsequences and only their per-SDS sums and u64 tallies are added at
+    the end.  weak: every rank walks `photons` photons (ranges rank*photons
+    ...); strong: the ranks split `photons`.  A rank never uses more
+    subsequences than it has photons, so starting each range at the rank's
+    first photon index keeps the ranges disjoint."""
+    if weak:
+        return rank * photons, photons
+    base, extra = divmod(photons, world)
+    n = base + (1 if rank < extra else 0)
+    return rank * base + min(rank, extra), n
 
 
 def uniform_stream(seed: int, subsequence: int, count: int, device: int = 0) -> np.ndarray:

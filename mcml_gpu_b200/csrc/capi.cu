@@ -245,6 +245,7 @@ int fill_result(mcml_ctx *c, mcml_result *r) {
   const double *wsq = reinterpret_cast<const double *>(sums + 64);
   r->num_sds = c->sim.num_sds;
   r->photons = c->N;
+  r->slots = c->S;
   r->steps = cnt[kCntSteps];
   const double Nd = (double)c->N;
   const double scale1 = (double)0xFFFFFFFF * Nd;

@@ -1,0 +1,152 @@
+"""Host-side logic without a GPU: the C ABI's exports, the configuration
+reader (read_mua_mus, io.cpp:35-256), the derived constants
+(io.cpp:168-238), the CLI's flag rules (main.cu:31-100) and the errors a
+caller gets without a device."""
+import json
+import math
+import re
+import subprocess
+import tempfile
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from conftest import CONFIGS, ROOT, load_case
+
+import mcml_gpu_b200 as m
+
+HEADER = ROOT / "include" / "mcml_b200.h"
+CLI = ROOT / "mcml_gpu_b200" / "bin" / "MCML_GPU"
+
+
+def declared_entry_points():
+    text = HEADER.read_text()
+    return sorted(set(re.findall(r"\b(mcml_[a-z_0-9]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_entry_point():
+    lib = m.load_library()
+    names = declared_entry_points()
+    assert len(names) >= 20
+    for n in names:
+        assert hasattr(lib, n), n
+    # the Python binding covers the whole header
+    assert set(names) == set(m.exported_symbols())
+
+
+def test_version_and_strerror():
+    lib = m.load_library()
+    assert b"K3.02" in lib.mcml_version()
+    assert lib.mcml_strerror(-4) == b"detection record buffer overflow"
+    assert lib.mcml_strerror(0) == b"ok"
+
+
+def test_parse_reference_example():
+    sim = load_case("c0")
+    assert sim.num_layers == 3 and sim.num_sds == 3
+    assert sim.number_photons == 1000000
+    assert sim.source_probe_oblique == 1 and sim.detector_probe_oblique == 1
+    np.testing.assert_array_equal(np.array(sim.mua[:3], np.float32),
+                                  np.array([0.3201, 0.2954, 0.2747], np.float32))
+    assert np.float32(sim.det_pos[1]) == np.float32(1.5)
+
+
+def test_derived_constants():
+    sim = load_case("c0")
+    d = m.derive(sim)
+    # Fresnel start weight at normal incidence, 1.457 -> 1.4 (io.cpp:230-237)
+    r = ((1.457 - 1.4) / (1.457 + 1.4)) ** 2
+    n0, n1 = float(np.float32(1.457)), float(np.float32(1.4))
+    r = ((n0 - n1) / (n0 + n1)) ** 2
+    assert d.start_weight == np.float32(int(0xFFFFFFFF * (1 - r)))
+    # layer stack with the 10 cm floor (io.cpp:107, 210-225)
+    assert np.float32(d.z_min[1]) == 0.0 and np.float32(d.z_max[1]) == np.float32(0.27)
+    assert np.float32(d.z_max[3]) == np.float32(10.0)
+    # 1/(mua+mus) in float
+    assert np.float32(d.mutr[1]) == np.float32(1.0) / (np.float32(0.3201) + np.float32(35.2861))
+    # critical angle asin(NA/upper_n) (io.cpp:196)
+    assert abs(d.critical_angle[1] - math.asin(0.13 / 1.457)) < 1e-6
+
+
+def _write_case(td, sim_json, input_txt):
+    (Path(td) / "s.json").write_text(json.dumps(sim_json))
+    (Path(td) / "in.txt").write_text(input_txt)
+    return Path(td) / "s.json", Path(td) / "in.txt"
+
+
+BASE = json.loads((CONFIGS / "c0" / "sim_set.json").read_text())
+GOOD_INPUT = (CONFIGS / "c0" / "input.txt").read_text()
+
+
+@pytest.mark.parametrize("edit,text,message", [
+    ({"source_probe_oblique": 2}, GOOD_INPUT, "source_probe_oblique: 2is not 1 or 0!"),
+    ({"detector_reflectance": 1.5}, GOOD_INPUT, "Detector reflectance: 1.5 is out of range !"),
+    ({"number_layers": 11}, GOOD_INPUT, "Number of layer is too large!"),
+    ({"probes": dict(BASE["probes"], num_SDS=2)}, GOOD_INPUT,
+     "Number of SDS : 2 not match the probe setting : 3 !"),
+    ({}, "0.27 0.3 35 1.4 0 0.65 0.3 30 1.4 0 0.27 0 1.4 0", "Mus for simulation 0 layer 2"),
+    ({}, "0.27 0.3 35 1.4 0 0.65 0.3 30 1.4 0 0.27 130 1.0 0", "n for simulation 0 layer 2"),
+    ({}, "0.27 0.3 35 1.4 0 0.65 0.3 30 1.4 0 0.27 130 1.4 1.5", "g for simulation 0 layer 2"),
+    ({}, "0.27 0.3 35", "Mus for simulation 0 layer 2 Error with value 0 !"),
+])
+def test_config_errors_carry_reference_messages(edit, text, message):
+    with tempfile.TemporaryDirectory() as td:
+        sj, it = _write_case(td, dict(BASE, **edit), text)
+        with pytest.raises(m.MCMLError) as e:
+            m.parse_config(sj, it)
+        assert message in e.value.message
+
+
+def test_multi_simulation_file():
+    with tempfile.TemporaryDirectory() as td:
+        sj, it = _write_case(td, dict(BASE, number_simulation=2),
+                             GOOD_INPUT.strip() + "\n" + GOOD_INPUT.replace("0.3201", "0.5"))
+        sims = m.parse_config(sj, it)
+        assert len(sims) == 2
+        assert np.float32(sims[1].mua[0]) == np.float32(0.5)
+
+
+def test_create_without_gpu_fails_cleanly():
+    if m.device_count() > 0:
+        pytest.skip("a GPU is present")
+    sim = load_case("c0")
+    with pytest.raises(m.MCMLError) as e:
+        m.Simulation(sim)
+    assert e.value.status == -9  # MCML_E_NODEV
+
+
+def test_invalid_sim_rejected_before_device_use():
+    sim = load_case("c0")
+    sim.num_layers = 11
+    with pytest.raises(m.MCMLError) as e:
+        m.Simulation(sim)
+    assert e.value.status == -1
+
+
+def run_cli(*args, cwd=None):
+    return subprocess.run([str(CLI), *args], capture_output=True, text=True, cwd=cwd, timeout=60)
+
+
+def test_cli_usage_and_flag_rules():
+    r = run_cli()
+    assert r.returncode == 0 and "Usage:" in r.stderr
+    sj, it = CONFIGS / "c0" / "sim_set.json", CONFIGS / "c0" / "input.txt"
+    for flags, msg in [(["-P"], "-P option only work with -R option!"),
+                       (["-A"], "-A option only work with -R option!"),
+                       (["-AP"], "-AP option only work with -R option!"),
+                       (["-R", "-B"], None),
+                       (["-B"], "-B option only work with -P or -A option!")]:
+        r = run_cli(str(sj), str(it), "out.txt", *flags, cwd=tempfile.gettempdir())
+        if msg:
+            assert r.returncode == 0 and msg in r.stdout, (flags, r.stdout)
+    r = run_cli(str(sj), str(it), "out.txt", "-G", "-1")
+    assert r.returncode == 0 and "GPU selection ERROR!" in r.stdout
+
+
+def test_cli_bad_config_exits_1():
+    with tempfile.TemporaryDirectory() as td:
+        sj, it = _write_case(td, dict(BASE, detector_reflectance=2.0), GOOD_INPUT)
+        r = run_cli(str(sj), str(it), "out.txt", cwd=td)
+        assert r.returncode == 1
+        assert "Something wrong with read_simulation_data!" in r.stdout
