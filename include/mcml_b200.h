@@ -238,6 +238,42 @@ int mcml_average_pathlength(mcml_ctx *ctx, double *out);
 int mcml_write_outputs(mcml_ctx *ctx, const char *dir, const char *output_txt,
                        uint32_t flags, double sim_s, double replay_s);
 
+/* ---- first pass without device allocation ----------------------------- */
+/*
+ * No counterpart in the reference (its host allocates with cudaMalloc on
+ * every run, transport.cu:1037-1097).  For callers that cannot allocate
+ * device memory when they want photons walked: code recording a CUDA graph
+ * (allocation is not allowed during stream capture and would synchronise
+ * the device), real-time pipelines whose device memory is fixed at
+ * start-up, or processes whose GPU memory another framework's pool owns.
+ *
+ * The walk's scratch memory is a fixed array of MCML_NOALLOC_SCRATCH_BYTES
+ * inside the library, present on every GPU that loads it until the process
+ * exits; it holds at most MCML_NOALLOC_MAX_SLOTS slot states, enough for the
+ * reference's one-photon-per-thread layout on a B200 (303104).  The call
+ * enqueues the first pass on `stream` (NULL = the legacy default stream)
+ * and returns without waiting; *out (a DEVICE pointer the caller owns)
+ * receives the per-SDS counts and FP64 weight sums when the stream reaches
+ * it.  slots = 0 picks min(N, MCML_NOALLOC_MAX_SLOTS); larger values are
+ * rejected with MCML_E_INVALID.  The same seed and slots give the same
+ * counts as mcml_run.  No detection records are kept (use mcml_run for the
+ * replay).  The first call on a device does its set-up (it looks up the
+ * array's device address), so make that call before any stream capture.
+ * All calls share the one array, which keeps the last call's contents;
+ * each call clears what must start at zero, and calls that overlap on the
+ * GPU (different streams or host threads) race -- serialise them.
+ */
+#define MCML_NOALLOC_SCRATCH_BYTES (8u << 20)
+#define MCML_NOALLOC_MAX_SLOTS ((MCML_NOALLOC_SCRATCH_BYTES - 1024u) / 24u)
+typedef struct mcml_noalloc_result {
+  uint64_t detected[MCML_MAX_SDS];
+  double weight_sum[MCML_MAX_SDS];
+  double weight_sumsq[MCML_MAX_SDS];
+  uint64_t steps;
+} mcml_noalloc_result;
+int mcml_run_noalloc(const mcml_sim *sim, uint64_t seed, uint64_t slots, int device,
+                     void *stream, mcml_noalloc_result *out);
+
 /* ---- test support ------------------------------------------------------ */
 /*
  * The first count draws of curand_uniform on the XORWOW state

@@ -144,6 +144,16 @@ class DeviceInfo(C.Structure):
     ]
 
 
+class NoallocResult(C.Structure):
+    """mcml_noalloc_result, written to device memory by mcml_run_noalloc."""
+    _fields_ = [
+        ("detected", C.c_uint64 * MAX_SDS),
+        ("weight_sum", C.c_double * MAX_SDS),
+        ("weight_sumsq", C.c_double * MAX_SDS),
+        ("steps", C.c_uint64),
+    ]
+
+
 _lib: Optional[C.CDLL] = None
 
 # (name, restype, argtypes) of every entry point of include/mcml_b200.h
@@ -174,6 +184,8 @@ _SIGNATURES = [
                                      C.c_double, C.c_double]),
     ("mcml_uniform_stream", C.c_int, [C.c_int, C.c_uint64, C.c_uint64, C.c_uint64,
                                       C.c_void_p]),
+    ("mcml_run_noalloc", C.c_int, [C.POINTER(Sim), C.c_uint64, C.c_uint64, C.c_int,
+                                   C.c_void_p, C.c_void_p]),
 ]
 
 

@@ -30,7 +30,7 @@ NVCC_FLAGS = ARCH + [
     "-I", str(ROOT / "include"),
 ]
 
-LIB_SOURCES = ["kernels.cu", "capi.cu", "config.cpp", "writers.cpp"]
+LIB_SOURCES = ["kernels.cu", "capi.cu", "config.cpp", "writers.cpp", "noalloc.cu"]
 HEADERS = ["photon.cuh", "kernels.h", "internal.h", "json_min.h"]
 
 
