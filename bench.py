@@ -227,6 +227,56 @@ def reference_gpu_arm(args) -> int:
     return 0
 
 
+def batch_arm(args) -> int:
+    """Config 2: 4096 parameter sets of the 5-layer tissue (mua, mus drawn
+    from config 1's ranges by seed, photons log-uniform 1e5-1e7 per set) in
+    one persistent CUDA-graph launch, autotuned; compared with the same sets
+    run one after another (a sample of them, rate extrapolated)."""
+    import torch
+    import mcml_gpu_b200 as m
+    base = load_sim(None)
+    n_sets = args.sets
+    sims = m.sample_sets(base, n_sets, seed=20261203, photons=(args.min_photons, args.max_photons))
+    total = sum(int(s.number_photons) for s in sims)
+    with m.Batch(sims, seed=args.seed) as b:
+        t0 = time.perf_counter()
+        tuning = b.autotune(1 / 64)
+        tune_s = time.perf_counter() - t0
+        for _ in range(max(args.warmup, 1)):
+            b.run()
+        times = []
+        for _ in range(args.steps):
+            res = b.run()
+            times.append(res[0].walk_ms)
+    ms = sum(times) / len(times)
+    steps = sum(int(r.steps) for r in res)
+    # the same sets one at a time through mcml_run (sample of 32 sets)
+    sample = sims[:: max(1, n_sets // 32)][:32]
+    seq_photons, seq_ms = 0, 0.0
+    for i, s in enumerate(sample):
+        with m.Simulation(s, seed=args.seed + i) as run:
+            run.run()
+            t0 = time.perf_counter()
+            run.run()
+            seq_ms += 1000 * (time.perf_counter() - t0)
+            seq_photons += int(s.number_photons)
+    rel = [r.std_error[1] / r.reflectance[1] for r in res if r.reflectance[1] > 0]
+    print(json.dumps({
+        "metric": "photons/s (batched plain MC)", "impl": "mcml-batch", "value": total / (ms / 1e3),
+        "unit": "photons/s", "ms_per_step": ms, "steps": args.steps, "warmup": args.warmup,
+        "config": {"workload": "config 2: batched 5-layer sets, log-uniform photons per set",
+                   "sets": n_sets, "photons_total": total,
+                   "photons_per_set": [args.min_photons, args.max_photons],
+                   "tuned": {"block": tuning.block_size, "blocks_per_sm": tuning.blocks_per_sm,
+                             "photons_per_slot": tuning.photons_per_slot},
+                   "tune_s": round(tune_s, 2), "cuda_graph": True},
+        "steps_per_s": steps / (ms / 1e3),
+        "sequential_same_library": {"value": seq_photons / (seq_ms / 1e3), "sets": len(sample)},
+        "median_rel_se_sds2": float(np.median(rel)) if rel else None,
+    }), flush=True)
+    return 0
+
+
 def read_traffic(slots: int) -> float | None:
     """DRAM bytes of one walk launch: the ncu-measured bytes per slot of a
     smaller capture (profiles/walk_kernel_traffic.json) times this run's
@@ -383,7 +433,8 @@ def main() -> int:
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", choices=["mcml", "reference", "reference-gpu"], default="mcml")
+    ap.add_argument("--impl", choices=["mcml", "reference", "reference-gpu", "batch"],
+                    default="mcml")
     ap.add_argument("--photons", type=int, default=0, help="override N (default: 1e8)")
     ap.add_argument("--slots", type=int, default=0)
     ap.add_argument("--block", type=int, default=0)
@@ -392,11 +443,16 @@ def main() -> int:
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-sample", type=int, default=300000)
+    ap.add_argument("--sets", type=int, default=4096)
+    ap.add_argument("--min-photons", type=float, default=1e5)
+    ap.add_argument("--max-photons", type=float, default=1e7)
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
     if args.impl == "reference-gpu":
         return reference_gpu_arm(args)
+    if args.impl == "batch":
+        return batch_arm(args)
     return mcml_arm(args)
 
 

@@ -238,6 +238,48 @@ int mcml_average_pathlength(mcml_ctx *ctx, double *out);
 int mcml_write_outputs(mcml_ctx *ctx, const char *dir, const char *output_txt,
                        uint32_t flags, double sim_s, double replay_s);
 
+/* ---- batches of parameter sets ---------------------------------------- */
+/*
+ * Many tissue parameter sets in one persistent launch.  Replaces running
+ * the reference once per set (its multi-simulation mode shares one
+ * critical-angle table, io.cpp:193-197).  Set b (sims[b], with its own
+ * number_photons) walks on ceil(N_b / photons_per_slot) slots of seed
+ * seed + b -- the same photons as mcml_run on that set alone with that
+ * seed and slot count, so per-set results are identical.  All sets need
+ * the same source/detector modes.  The seeding and the walk are captured
+ * into a CUDA graph on the first run and relaunched afterwards.  Results:
+ * one mcml_result per set (counts, FP64 weight sums, reflectance and its
+ * standard error; no replay).
+ */
+typedef struct mcml_batch_opts {
+  uint64_t seed;              /* set b uses seed + b                          */
+  int32_t device;
+  uint32_t photons_per_slot;  /* 0 = 64                                       */
+  uint32_t block_size;        /* 0 = default walk variant                     */
+  uint32_t blocks_per_sm;
+  void *stream;               /* NULL = a library stream (graphs cannot be
+                                 captured on the legacy default stream)      */
+  int32_t no_graph;           /* 1: plain launches instead of a CUDA graph    */
+} mcml_batch_opts;
+
+typedef struct mcml_batch_tuning {
+  uint32_t block_size;
+  uint32_t blocks_per_sm;
+  uint32_t photons_per_slot;
+  float pilot_ms;
+} mcml_batch_tuning;
+
+typedef struct mcml_batch mcml_batch;
+int mcml_batch_create(const mcml_sim *sims, int num_sets, const mcml_batch_opts *opts,
+                      mcml_batch **batch);
+/* Times pilot runs (photon_fraction of each set's photons) over the walk
+ * variants and photons-per-slot choices and keeps the fastest. */
+int mcml_batch_autotune(mcml_batch *batch, double photon_fraction, mcml_batch_tuning *chosen);
+int mcml_batch_run(mcml_batch *batch, mcml_result *results);
+int mcml_batch_launch(mcml_batch *batch);
+int mcml_batch_get_results(mcml_batch *batch, mcml_result *results);
+void mcml_batch_destroy(mcml_batch *batch);
+
 /* ---- first pass without device allocation ----------------------------- */
 /*
  * No counterpart in the reference (its host allocates with cudaMalloc on

@@ -22,7 +22,8 @@ import numpy as np
 __all__ = [
     "MAX_LAYERS", "MAX_SDS", "MCMLError", "Sim", "Opts", "Result", "Derived",
     "DeviceInfo", "load_library", "lib_path", "parse_config", "derive", "make_sim",
-    "Simulation", "uniform_stream", "device_count", "device_info",
+    "Simulation", "Batch", "sample_sets", "shard", "uniform_stream", "device_count",
+    "device_info",
     "OUT_REPLAY", "OUT_ABSORBANCE", "OUT_PATHLENGTH", "OUT_AVERAGE_PL", "OUT_BINARY",
 ]
 
@@ -154,6 +155,27 @@ class NoallocResult(C.Structure):
     ]
 
 
+class BatchOpts(C.Structure):
+    _fields_ = [
+        ("seed", C.c_uint64),
+        ("device", C.c_int32),
+        ("photons_per_slot", C.c_uint32),
+        ("block_size", C.c_uint32),
+        ("blocks_per_sm", C.c_uint32),
+        ("stream", C.c_void_p),
+        ("no_graph", C.c_int32),
+    ]
+
+
+class BatchTuning(C.Structure):
+    _fields_ = [
+        ("block_size", C.c_uint32),
+        ("blocks_per_sm", C.c_uint32),
+        ("photons_per_slot", C.c_uint32),
+        ("pilot_ms", C.c_float),
+    ]
+
+
 _lib: Optional[C.CDLL] = None
 
 # (name, restype, argtypes) of every entry point of include/mcml_b200.h
@@ -186,6 +208,13 @@ _SIGNATURES = [
                                       C.c_void_p]),
     ("mcml_run_noalloc", C.c_int, [C.POINTER(Sim), C.c_uint64, C.c_uint64, C.c_int,
                                    C.c_void_p, C.c_void_p]),
+    ("mcml_batch_create", C.c_int, [C.c_void_p, C.c_int, C.POINTER(BatchOpts),
+                                    C.POINTER(C.c_void_p)]),
+    ("mcml_batch_autotune", C.c_int, [C.c_void_p, C.c_double, C.POINTER(BatchTuning)]),
+    ("mcml_batch_run", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("mcml_batch_launch", C.c_int, [C.c_void_p]),
+    ("mcml_batch_get_results", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("mcml_batch_destroy", None, [C.c_void_p]),
 ]
 
 
@@ -422,3 +451,80 @@ class Simulation:
             self.close()
         except Exception:
             pass
+
+
+class Batch:
+    """Many parameter sets in one persistent launch (mcml_batch_*).  Set b
+    walks ceil(N_b / photons_per_slot) slots of seed + b, the same photons
+    as Simulation(sims[b], seed=seed + b, slots=...) alone."""
+
+    def __init__(self, sims: Sequence[Sim], *, seed: int = 0, device: int = 0,
+                 photons_per_slot: int = 0, block_size: int = 0, blocks_per_sm: int = 0,
+                 stream: Optional[int] = None, graph: bool = True):
+        self._lib = load_library()
+        self.sims = (Sim * len(sims))(*sims)
+        o = BatchOpts()
+        o.seed = seed
+        o.device = device
+        o.photons_per_slot = photons_per_slot
+        o.block_size = block_size
+        o.blocks_per_sm = blocks_per_sm
+        o.stream = stream
+        o.no_graph = 0 if graph else 1
+        self._b = C.c_void_p()
+        _check(self._lib.mcml_batch_create(self.sims, len(sims), C.byref(o), C.byref(self._b)),
+               "mcml_batch_create")
+
+    def autotune(self, photon_fraction: float = 1 / 16) -> BatchTuning:
+        t = BatchTuning()
+        _check(self._lib.mcml_batch_autotune(self._b, photon_fraction, C.byref(t)),
+               "mcml_batch_autotune")
+        return t
+
+    def run(self) -> list:
+        res = (Result * len(self.sims))()
+        _check(self._lib.mcml_batch_run(self._b, res), "mcml_batch_run")
+        return list(res)
+
+    def launch(self) -> None:
+        _check(self._lib.mcml_batch_launch(self._b), "mcml_batch_launch")
+
+    def results(self) -> list:
+        res = (Result * len(self.sims))()
+        _check(self._lib.mcml_batch_get_results(self._b, res), "mcml_batch_get_results")
+        return list(res)
+
+    def close(self) -> None:
+        if getattr(self, "_b", None) and self._b.value:
+            self._lib.mcml_batch_destroy(self._b)
+            self._b = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def sample_sets(base: Sim, count: int, seed: int, *, mua=(0.05, 0.5), mus=(50.0, 250.0),
+                photons=(1e5, 1e7)) -> list:
+    """Parameter sets for a batch: `base`'s geometry with per-layer mua and
+    mus drawn uniformly and per-set photon counts drawn log-uniformly, from a
+    seeded generator (numpy PCG64)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    L = int(base.num_layers)
+    for _ in range(count):
+        s = Sim.from_buffer_copy(base)
+        for l in range(L):
+            s.mua[l] = float(rng.uniform(*mua))
+            s.mus[l] = float(rng.uniform(*mus))
+        s.number_photons = int(round(10 ** rng.uniform(np.log10(photons[0]), np.log10(photons[1]))))
+        out.append(s)
+    return out

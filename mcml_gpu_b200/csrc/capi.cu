@@ -17,6 +17,7 @@
 #include "../../include/mcml_b200.h"
 #include "internal.h"
 #include "kernels.h"
+#include "params.h"
 
 namespace mcml {
 
@@ -137,44 +138,11 @@ bool ref_grid(const mcml_ctx *c) {
 }
 
 int build_params(mcml_ctx *c) {
-  const mcml_sim &s = c->sim;
-  const mcml_derived &d = c->der;
-  DevParams &P = c->P;
-  std::memset(&P, 0, sizeof(P));
-  const int L = (int)s.num_layers;
-  for (int l = 0; l <= L + 1; ++l) {
-    P.z_min[l] = d.z_min[l];
-    P.z_max[l] = d.z_max[l];
-    P.mutr[l] = d.mutr[l];
-    if (l >= 1 && l <= L) {
-      P.mua[l] = s.mua[l - 1];
-      P.g[l] = s.g[l - 1];
-      P.n[l] = s.n[l - 1];
-    }
-  }
-  P.n[0] = s.upper_n;
-  P.n[L + 1] = s.lower_n;
-  P.det_radius[0] = s.source_radius;
-  P.det_NA[0] = s.source_NA;
-  P.det_pos[0] = 0.0f;
-  P.det_angle[0] = d.det_angle_rad[0];
-  for (unsigned i = 0; i < s.num_sds; ++i) {
-    P.det_radius[i + 1] = s.det_radius[i];
-    P.det_NA[i + 1] = s.det_NA[i];
-    P.det_pos[i + 1] = s.det_pos[i];
-    P.det_angle[i + 1] = d.det_angle_rad[i + 1];
-    P.crit[i + 1] = d.critical_angle[i + 1];
-  }
-  P.n_layers = s.num_layers;
-  P.n_sds = s.num_sds;
-  P.start_weight = d.start_weight;
-  P.det_reflectance = s.detector_reflectance;
-  P.num_photons = c->N;
-  P.num_slots = c->S;
-  P.grid_nr = grid_nr(c);
-  P.grid_nz = grid_nz(c);
-  P.grid_dr = grid_dr(c);
-  P.grid_dz = grid_dz(c);
+  fill_dev_params(c->sim, c->der, c->N, c->S, c->P);
+  c->P.grid_nr = grid_nr(c);
+  c->P.grid_nz = grid_nz(c);
+  c->P.grid_dr = grid_dr(c);
+  c->P.grid_dz = grid_dz(c);
   return MCML_OK;
 }
 
