@@ -280,6 +280,32 @@ int mcml_batch_launch(mcml_batch *batch);
 int mcml_batch_get_results(mcml_batch *batch, mcml_result *results);
 void mcml_batch_destroy(mcml_batch *batch);
 
+/* ---- White Monte Carlo relabelling ------------------------------------ */
+/*
+ * Reflectance of one SDS under other absorption / scattering coefficients,
+ * from one replay: each combo c gives
+ *   R_c = sum_i w_i prod_l (mus'_l/mus_l)^n_il exp(-sum_l (dmua_l+dmus_l) PL_il) / scale
+ * over the SDS's replayed photons i (weight w, pathlengths PL, interaction
+ * counts n from mcml_get_rows).  The mua-only case is the factor of
+ * calculate_average_pathlength (transport.cu:285-292); the mus factor
+ * needs the interaction counts the reference does not record.
+ * All arrays are DEVICE pointers; work is enqueued on `stream`.
+ */
+typedef struct mcml_wmc_set {
+  const float *pathlength;   /* L x D, layer-major: PL of photon i in layer l at [l*D+i] */
+  const float *interactions; /* L x D, layer-major, interaction counts as float       */
+  const float *weight;       /* D detected weights (quanta)                            */
+  uint64_t count;            /* D                                                      */
+  uint32_t num_layers;       /* L                                                      */
+} mcml_wmc_set;
+uint64_t mcml_wmc_workspace_bytes(uint64_t num_photons, uint64_t num_combos);
+/* base_mua/base_mus: HOST, L each (the replayed run's coefficients).
+ * combos: C x 2L (mua'_1..L, mus'_1..L).  scale: 0xFFFFFFFF * N of the run.
+ * out: C doubles.  workspace: mcml_wmc_workspace_bytes(D, C) device bytes. */
+int mcml_wmc_rescale(const mcml_wmc_set *set, const float *base_mua, const float *base_mus,
+                     const float *combos, uint64_t num_combos, double scale, double *out,
+                     void *workspace, uint64_t workspace_bytes, void *stream);
+
 /* ---- first pass without device allocation ----------------------------- */
 /*
  * No counterpart in the reference (its host allocates with cudaMalloc on

@@ -30,7 +30,8 @@ NVCC_FLAGS = ARCH + [
     "-I", str(ROOT / "include"),
 ]
 
-LIB_SOURCES = ["kernels.cu", "capi.cu", "config.cpp", "writers.cpp", "noalloc.cu", "batch.cu"]
+LIB_SOURCES = ["kernels.cu", "capi.cu", "config.cpp", "writers.cpp", "noalloc.cu", "batch.cu",
+               "wmc.cu"]
 HEADERS = ["photon.cuh", "kernels.h", "internal.h", "json_min.h", "params.h"]
 
 

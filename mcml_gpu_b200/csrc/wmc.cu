@@ -1,0 +1,201 @@
+// wmc.cu -- White Monte Carlo relabelling of replayed photons.
+//
+// A replayed photon's detected weight w, per-layer pathlengths PL_l and
+// per-layer interaction counts n_l determine its weight under other
+// optical coefficients without walking again.  In this walk the step length
+// is drawn from mu_t = mu_a + mu_s and each interaction keeps the fraction
+// mu_s/mu_t of the weight, so the path's contribution is proportional to
+// prod_l mu_s_l^n_l exp(-mu_t_l PL_l); changing (mu_a, mu_s) to
+// (mu_a', mu_s') multiplies it by
+//
+//     prod_l (mu_s'_l / mu_s_l)^n_l * exp(-sum_l (mu_t'_l - mu_t_l) PL_l).
+//
+// For mu_a alone this is exp(-sum dmu_a PL), the factor the reference uses
+// for its average pathlength (transport.cu:285-292); the mu_s factor needs
+// the interaction counts, which the reference does not record and this
+// library's replay does.  Roulette and the integer weight quanta make the
+// rescaled estimate unbiased in expectation, as White MC always is.
+//
+// Per (combo c, photon i) the kernel evaluates
+//     R_c += exp2( sum_k a_ck F_ik ),   F_i = [PL_1..L, n_1..L, log2 w_i, 1]
+// with a_c = [-(dmu_t)*log2(e) ..., log2(mu_s'/mu_s) ..., 1, 0]: a K=2L+2
+// contraction, one exp2 (MUFU) and one add.  The exponents reach hundreds,
+// so the contraction stays in FP32 on the CUDA cores (a bf16/tf32 tensor
+// product would lose the exponent's low bits).  Photon features are staged
+// through shared memory in chunks and each thread carries kPer combos.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <string>
+
+#include "../../include/mcml_b200.h"
+#include "internal.h"
+
+namespace mcml {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kPer = 4;      // combos per thread
+constexpr int kChunk = 256;  // photons per shared-memory chunk
+constexpr int kMaxK = 2 * MCML_MAX_LAYERS + 2;
+
+// Packs F_i (k-major within a photon, padded to kMaxK) for every photon.
+__global__ void wmc_pack_kernel(const float *pl, const float *inter, const float *w,
+                                uint64_t D, int L, float *F) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= D) return;
+  float *f = F + i * kMaxK;
+  for (int l = 0; l < L; ++l) {
+    f[l] = pl[(uint64_t)l * D + i];
+    f[L + l] = inter[(uint64_t)l * D + i];
+  }
+  const float wi = w[i];
+  f[2 * L] = wi > 0.0f ? log2f(wi) : -INFINITY;
+  f[2 * L + 1] = 1.0f;
+  for (int k = 2 * L + 2; k < kMaxK; ++k) f[k] = 0.0f;
+}
+
+template <int K>
+__global__ void __launch_bounds__(kThreads) wmc_kernel(const float *F, uint64_t D,
+                                                       const float *coef, uint64_t C,
+                                                       double inv_scale, double *out) {
+  __shared__ float sF[kChunk][K];
+  const uint64_t c0 = ((uint64_t)blockIdx.x * kThreads + threadIdx.x) * kPer;
+  float a[kPer][K];
+#pragma unroll
+  for (int r = 0; r < kPer; ++r)
+#pragma unroll
+    for (int k = 0; k < K; ++k) a[r][k] = (c0 + r < C) ? coef[(c0 + r) * kMaxK + k] : 0.0f;
+  double total[kPer];
+#pragma unroll
+  for (int r = 0; r < kPer; ++r) total[r] = 0.0;
+
+  for (uint64_t base = 0; base < D; base += kChunk) {
+    const int n = (int)((D - base) < (uint64_t)kChunk ? (D - base) : (uint64_t)kChunk);
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < n * K; idx += kThreads) {
+      const int j = idx / K, k = idx % K;
+      sF[j][k] = F[(base + j) * kMaxK + k];
+    }
+    __syncthreads();
+    float acc[kPer];
+#pragma unroll
+    for (int r = 0; r < kPer; ++r) acc[r] = 0.0f;
+    for (int j = 0; j < n; ++j) {
+      float e[kPer];
+#pragma unroll
+      for (int r = 0; r < kPer; ++r) e[r] = 0.0f;
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        const float f = sF[j][k];
+#pragma unroll
+        for (int r = 0; r < kPer; ++r) e[r] = fmaf(a[r][k], f, e[r]);
+      }
+#pragma unroll
+      for (int r = 0; r < kPer; ++r) acc[r] += exp2f(e[r]);
+    }
+#pragma unroll
+    for (int r = 0; r < kPer; ++r) total[r] += (double)acc[r];
+  }
+#pragma unroll
+  for (int r = 0; r < kPer; ++r)
+    if (c0 + r < C) out[c0 + r] = total[r] * inv_scale;
+}
+
+// Per-combo coefficient rows a_c (padded to kMaxK).
+__global__ void wmc_coef_kernel(const float *combos, uint64_t C, int L, const float *base,
+                                float *coef) {
+  const uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= C) return;
+  const float *x = combos + c * 2 * L;  // mua'_1..L, mus'_1..L
+  float *a = coef + c * kMaxK;
+  const float log2e = 1.4426950408889634f;
+  for (int l = 0; l < L; ++l) {
+    const float dmut = (x[l] - base[l]) + (x[L + l] - base[L + l]);
+    a[l] = -dmut * log2e;
+    a[L + l] = log2f(x[L + l] / base[L + l]);
+  }
+  a[2 * L] = 1.0f;
+  a[2 * L + 1] = 0.0f;
+  for (int k = 2 * L + 2; k < kMaxK; ++k) a[k] = 0.0f;
+}
+
+template <int K>
+cudaError_t launch_wmc(const float *F, uint64_t D, const float *coef, uint64_t C,
+                       double inv_scale, double *out, cudaStream_t s) {
+  const uint64_t per_block = (uint64_t)kThreads * kPer;
+  const unsigned grid = (unsigned)((C + per_block - 1) / per_block);
+  wmc_kernel<K><<<grid, kThreads, 0, s>>>(F, D, coef, C, inv_scale, out);
+  return cudaGetLastError();
+}
+
+}  // namespace
+}  // namespace mcml
+
+using namespace mcml;
+
+extern "C" int mcml_wmc_rescale(const mcml_wmc_set *set, const float *base_mua,
+                                const float *base_mus, const float *combos, uint64_t num_combos,
+                                double scale, double *out, void *workspace,
+                                uint64_t workspace_bytes, void *stream) {
+  clear_error();
+  if (!set || !base_mua || !base_mus || !combos || !out)
+    return set_error(MCML_E_INVALID, "mcml_wmc_rescale: null argument");
+  const int L = (int)set->num_layers;
+  if (L < 1 || L > MCML_MAX_LAYERS) return set_error(MCML_E_INVALID, "num_layers must be in [1,10]");
+  const uint64_t D = set->count;
+  const uint64_t need = mcml_wmc_workspace_bytes(D, num_combos);
+  if (!workspace || workspace_bytes < need)
+    return set_error(MCML_E_INVALID, "mcml_wmc_rescale: workspace of " + std::to_string(need) +
+                                         " bytes needed");
+  if (num_combos == 0) return MCML_OK;
+  if (!(scale > 0)) return set_error(MCML_E_INVALID, "scale must be > 0");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // workspace: base[2L] | coef[C x kMaxK] | F[D x kMaxK]
+  float *base = static_cast<float *>(workspace);
+  float *coef = base + 2 * MCML_MAX_LAYERS + 4;
+  float *F = coef + num_combos * kMaxK;
+  float hbase[2 * MCML_MAX_LAYERS];
+  for (int l = 0; l < L; ++l) {
+    hbase[l] = base_mua[l];
+    hbase[L + l] = base_mus[l];
+  }
+  cudaError_t e = cudaMemcpyAsync(base, hbase, 2 * L * sizeof(float), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) {
+    wmc_coef_kernel<<<(unsigned)((num_combos + 255) / 256), 256, 0, s>>>(combos, num_combos, L,
+                                                                         base, coef);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess && D > 0) {
+    wmc_pack_kernel<<<(unsigned)((D + 255) / 256), 256, 0, s>>>(set->pathlength, set->interactions,
+                                                                set->weight, D, L, F);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) {
+    const double inv = 1.0 / scale;
+    if (D == 0) {
+      e = cudaMemsetAsync(out, 0, num_combos * sizeof(double), s);
+    } else {
+      switch (2 * L + 2) {
+        case 4: e = launch_wmc<4>(F, D, coef, num_combos, inv, out, s); break;
+        case 6: e = launch_wmc<6>(F, D, coef, num_combos, inv, out, s); break;
+        case 8: e = launch_wmc<8>(F, D, coef, num_combos, inv, out, s); break;
+        case 10: e = launch_wmc<10>(F, D, coef, num_combos, inv, out, s); break;
+        case 12: e = launch_wmc<12>(F, D, coef, num_combos, inv, out, s); break;
+        case 14: e = launch_wmc<14>(F, D, coef, num_combos, inv, out, s); break;
+        case 16: e = launch_wmc<16>(F, D, coef, num_combos, inv, out, s); break;
+        case 18: e = launch_wmc<18>(F, D, coef, num_combos, inv, out, s); break;
+        case 20: e = launch_wmc<20>(F, D, coef, num_combos, inv, out, s); break;
+        default: e = launch_wmc<22>(F, D, coef, num_combos, inv, out, s); break;
+      }
+    }
+  }
+  if (e != cudaSuccess)
+    return set_error(MCML_E_CUDA, std::string("mcml_wmc_rescale: ") + cudaGetErrorString(e));
+  return MCML_OK;
+}
+
+extern "C" uint64_t mcml_wmc_workspace_bytes(uint64_t num_photons, uint64_t num_combos) {
+  return (uint64_t)(2 * MCML_MAX_LAYERS + 4) * sizeof(float) +
+         (num_combos + num_photons) * (uint64_t)(2 * MCML_MAX_LAYERS + 2) * sizeof(float);
+}
