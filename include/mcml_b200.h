@@ -306,6 +306,40 @@ int mcml_wmc_rescale(const mcml_wmc_set *set, const float *base_mua, const float
                      const float *combos, uint64_t num_combos, double scale, double *out,
                      void *workspace, uint64_t workspace_bytes, void *stream);
 
+/* ---- MLP surrogate ----------------------------------------------------- */
+/*
+ * No counterpart in the reference.  An ensemble of MLPs
+ * (in -> hidden x depth, GELU -> out) trained and evaluated by this
+ * library's BF16 tensor-core kernels with FP32 accumulation and FP32
+ * master weights (Adam).  Inputs and targets are normalised with
+ * mcml_mlp_set_normalization; predictions come back de-normalised with the
+ * ensemble's spread.  X, T, mean and spread are DEVICE arrays.
+ */
+typedef struct mcml_mlp_config {
+  int32_t in_dim, hidden, depth, out_dim, ensemble;
+  uint64_t seed;
+  int32_t device;
+  void *stream;
+} mcml_mlp_config;
+typedef struct mcml_mlp mcml_mlp;
+int mcml_mlp_create(const mcml_mlp_config *cfg, mcml_mlp **mlp);
+int mcml_mlp_set_normalization(mcml_mlp *mlp, const float *x_mean, const float *x_std,
+                               const float *t_mean, const float *t_std);
+int64_t mcml_mlp_num_params(const mcml_mlp *mlp);
+/* FP32 parameters of one member (host), layer by layer: W (fan_in x
+ * fan_out, row-major, fan_in of layer 0 padded to a multiple of 8) then b. */
+int mcml_mlp_get_params(mcml_mlp *mlp, float *host, int member);
+int mcml_mlp_set_params(mcml_mlp *mlp, const float *host, int member);
+/* Loss and gradients of every member on rows [0, n) (no update; host out). */
+int mcml_mlp_gradients(mcml_mlp *mlp, const float *X, const float *T, int n, float *loss,
+                       float *grads);
+int mcml_mlp_train_epoch(mcml_mlp *mlp, const float *X, const float *T, uint64_t n,
+                         uint32_t batch, float lr, uint64_t shuffle_seed, float *loss);
+int mcml_mlp_predict(mcml_mlp *mlp, const float *X, uint64_t n, float *mean, float *spread,
+                     uint32_t chunk);
+int mcml_mlp_sync(mcml_mlp *mlp);
+void mcml_mlp_destroy(mcml_mlp *mlp);
+
 /* ---- first pass without device allocation ----------------------------- */
 /*
  * No counterpart in the reference (its host allocates with cudaMalloc on

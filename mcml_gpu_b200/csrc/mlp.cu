@@ -1,0 +1,718 @@
+// mlp.cu -- BF16 MLP ensemble: training and inference kernels.
+//
+// The surrogate maps a tissue's layer parameters to per-SDS
+// log-reflectance.  Network: in -> hidden x depth (GELU) -> out, an
+// ensemble of E members trained side by side (gridDim.z = member).
+// Weights are kept in FP32 (master copy, Adam state) and mirrored to BF16
+// for the tensor-core GEMMs, which accumulate in FP32.
+//
+// GEMM: C[M x N] = op(A)[M x K] * op(B)[K x N], BF16 operands staged in
+// shared memory, mma.sync m16n8k16 fragments loaded with ldmatrix, FP32
+// accumulators, and a fused epilogue:
+//   kBiasGelu : Z = acc + bias (kept in FP32 for the backward pass),
+//               H = bf16(gelu(Z))
+//   kBias     : Y = acc + bias (FP32; the output layer)
+//   kGeluBack : dZ = bf16(acc * gelu'(Zprev))   (back through an activation)
+//   kStoreF32 : G = acc (FP32; weight gradients)
+// op(A) = A or A^T, op(B) = B or B^T by template flags, which gives the
+// backward products dW = H^T dZ and dH = dZ W^T from the same kernel.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "../../include/mcml_b200.h"
+#include "internal.h"
+
+namespace mcml {
+namespace {
+
+typedef __nv_bfloat16 bf16;
+
+constexpr int BM = 64, BN = 64, BK = 32;  // CTA tile
+constexpr int kGemmThreads = 128;         // 4 warps, 2 x 2, warp tile 32 x 32
+constexpr int PAD = 8;                    // smem row padding (bf16 elements)
+
+enum Epi { kBiasGelu = 0, kBias = 1, kGeluBack = 2, kStoreF32 = 3 };
+
+__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_grad(float z) {
+  const float cdf = 0.5f * (1.0f + erff(z * 0.70710678118654752f));
+  const float pdf = 0.39894228040143268f * __expf(-0.5f * z * z);
+  return cdf + z * pdf;
+}
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+
+struct GemmArgs {
+  int M, N, K;
+  const bf16 *A;
+  long long lda, strideA;  // per-member strides (elements)
+  const bf16 *B;
+  long long ldb, strideB;
+  const float *bias;       // [N] per member (kBiasGelu, kBias)
+  long long strideBias;
+  float *outF;             // FP32 output (Z for kBiasGelu, Y, G)
+  long long ldo, strideO;
+  bf16 *outH;              // BF16 output (H for kBiasGelu, dZ for kGeluBack)
+  long long ldh, strideH;
+  const float *aux;        // Zprev for kGeluBack
+  long long ldx, strideX;
+};
+
+template <bool TA, bool TB, int EPI>
+__global__ void __launch_bounds__(kGemmThreads) gemm_kernel(const GemmArgs g) {
+  __shared__ __align__(16) bf16 As[BM][BK + PAD];
+  __shared__ __align__(16) bf16 Bs[BK][BN + PAD];
+  const int z = blockIdx.z;
+  const bf16 *A = g.A + z * g.strideA;
+  const bf16 *B = g.B + z * g.strideB;
+  const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+  float acc[2][4][4];
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.0f;
+
+  for (int k0 = 0; k0 < g.K; k0 += BK) {
+    // A tile: As[m][k] = op(A)(m0+m, k0+k); consecutive threads read
+    // consecutive global addresses in either orientation.
+    for (int e = tid; e < BM * BK; e += kGemmThreads) {
+      int m, k;
+      if (TA) { m = e % BM; k = e / BM; } else { k = e % BK; m = e / BK; }
+      const int gm = m0 + m, gk = k0 + k;
+      bf16 v = __float2bfloat16(0.0f);
+      if (gm < g.M && gk < g.K) v = TA ? A[(long long)gk * g.lda + gm] : A[(long long)gm * g.lda + gk];
+      As[m][k] = v;
+    }
+    for (int e = tid; e < BK * BN; e += kGemmThreads) {
+      int k, n;
+      if (TB) { k = e % BK; n = e / BK; } else { n = e % BN; k = e / BN; }
+      const int gk = k0 + k, gn = n0 + n;
+      bf16 v = __float2bfloat16(0.0f);
+      if (gk < g.K && gn < g.N) v = TB ? B[(long long)gn * g.ldb + gk] : B[(long long)gk * g.ldb + gn];
+      Bs[k][n] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += 16) {
+      unsigned a[2][4], b[4][2];
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int row = wm + i * 16 + (lane & 15);
+        const int col = kk + (lane >> 4) * 8;
+        asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                     : "=r"(a[i][0]), "=r"(a[i][1]), "=r"(a[i][2]), "=r"(a[i][3])
+                     : "r"(smem_u32(&As[row][col])));
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int krow = kk + (lane & 15);
+        const int col = wn + j * 8;
+        asm volatile("ldmatrix.sync.aligned.m8n8.x2.trans.shared.b16 {%0,%1}, [%2];\n"
+                     : "=r"(b[j][0]), "=r"(b[j][1])
+                     : "r"(smem_u32(&Bs[krow][col])));
+      }
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          asm volatile(
+              "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
+              "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+              : "+f"(acc[i][j][0]), "+f"(acc[i][j][1]), "+f"(acc[i][j][2]), "+f"(acc[i][j][3])
+              : "r"(a[i][0]), "r"(a[i][1]), "r"(a[i][2]), "r"(a[i][3]), "r"(b[j][0]),
+                "r"(b[j][1]));
+    }
+    __syncthreads();
+  }
+
+  // Epilogue: thread holds rows (lane>>2) and (lane>>2)+8, columns 2*(lane&3)+{0,1}.
+  const float *bias = g.bias ? g.bias + z * g.strideBias : nullptr;
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int m = m0 + wm + i * 16 + (lane >> 2) + (r >= 2 ? 8 : 0);
+        const int n = n0 + wn + j * 8 + 2 * (lane & 3) + (r & 1);
+        if (m >= g.M || n >= g.N) continue;
+        const float v = acc[i][j][r];
+        if (EPI == kBiasGelu) {
+          const float zz = v + bias[n];
+          g.outF[z * g.strideO + (long long)m * g.ldo + n] = zz;
+          g.outH[z * g.strideH + (long long)m * g.ldh + n] = __float2bfloat16(gelu(zz));
+        } else if (EPI == kBias) {
+          g.outF[z * g.strideO + (long long)m * g.ldo + n] = v + bias[n];
+        } else if (EPI == kGeluBack) {
+          const float zp = g.aux[z * g.strideX + (long long)m * g.ldx + n];
+          g.outH[z * g.strideH + (long long)m * g.ldh + n] = __float2bfloat16(v * gelu_grad(zp));
+        } else {
+          g.outF[z * g.strideO + (long long)m * g.ldo + n] = v;
+        }
+      }
+}
+
+template <bool TA, bool TB, int EPI>
+cudaError_t gemm(const GemmArgs &g, int members, cudaStream_t s) {
+  dim3 grid((g.N + BN - 1) / BN, (g.M + BM - 1) / BM, members);
+  gemm_kernel<TA, TB, EPI><<<grid, kGemmThreads, 0, s>>>(g);
+  return cudaGetLastError();
+}
+
+// X rows of a minibatch -> BF16, normalised, zero-padded to in_pad columns.
+__global__ void gather_x_kernel(const float *X, const uint32_t *idx, int n, int in_dim, int in_pad,
+                                const float *mean, const float *inv_std, long long idx_stride,
+                                bf16 *out, long long out_stride) {
+  const int z = blockIdx.z;
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (long long)n * in_pad) return;
+  const int r = (int)(e / in_pad), c = (int)(e % in_pad);
+  float v = 0.0f;
+  if (c < in_dim) {
+    const uint32_t row = idx ? idx[z * idx_stride + r] : (uint32_t)r;
+    v = (X[(long long)row * in_dim + c] - mean[c]) * inv_std[c];
+  }
+  out[z * out_stride + e] = __float2bfloat16(v);
+}
+
+// Loss (mean squared error of normalised targets) and dY = 2 (Y - T) / (n * out).
+__global__ void loss_grad_kernel(const float *Yp, long long strideY, const float *T,
+                                 const uint32_t *idx, long long idx_stride, int n, int out_dim,
+                                 const float *tmean, const float *tinv, bf16 *dY,
+                                 long long strideD, float *loss) {
+  const int z = blockIdx.z;
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  float l = 0.0f;
+  if (e < (long long)n * out_dim) {
+    const int r = (int)(e / out_dim), c = (int)(e % out_dim);
+    const uint32_t row = idx[z * idx_stride + r];
+    const float t = (T[(long long)row * out_dim + c] - tmean[c]) * tinv[c];
+    const float d = Yp[z * strideY + e] - t;
+    l = d * d;
+    dY[z * strideD + e] = __float2bfloat16(2.0f * d / (float)((long long)n * out_dim));
+  }
+  for (int o = 16; o > 0; o >>= 1) l += __shfl_down_sync(0xffffffffu, l, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(&loss[z], l / (float)((long long)n * out_dim));
+}
+
+// db[j] = sum over rows of dZ[:, j] (BF16 in, FP32 out).
+__global__ void bias_grad_kernel(const bf16 *dZ, long long strideD, int n, int cols, float *db,
+                                 long long strideB) {
+  const int z = blockIdx.z;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= cols) return;
+  float s = 0.0f;
+  for (int r = 0; r < n; ++r) s += __bfloat162float(dZ[z * strideD + (long long)r * cols + c]);
+  db[z * strideB + c] = s;
+}
+
+// Adam on the FP32 master weights; refreshes the BF16 mirror.
+__global__ void adam_kernel(float *w, const float *grad, float *m, float *v, bf16 *w16,
+                            long long n, float lr, float b1, float b2, float eps, float c1,
+                            float c2) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float gr = grad[i];
+  const float mi = b1 * m[i] + (1.0f - b1) * gr;
+  const float vi = b2 * v[i] + (1.0f - b2) * gr * gr;
+  m[i] = mi;
+  v[i] = vi;
+  const float wi = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+  w[i] = wi;
+  if (w16) w16[i] = __float2bfloat16(wi);
+}
+
+__global__ void to_bf16_kernel(const float *x, bf16 *y, long long n) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] = __float2bfloat16(x[i]);
+}
+
+// Ensemble mean and standard deviation of de-normalised outputs.
+__global__ void ensemble_kernel(const float *Y, long long strideY, int E, long long n_out,
+                                const float *tmean, const float *tstd, int out_dim, float *mean,
+                                float *spread) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n_out) return;
+  const int c = (int)(e % out_dim);
+  float s = 0.0f, s2 = 0.0f;
+  for (int z = 0; z < E; ++z) {
+    const float y = Y[z * strideY + e] * tstd[c] + tmean[c];
+    s += y;
+    s2 += y * y;
+  }
+  const float mu = s / E;
+  mean[e] = mu;
+  if (spread) spread[e] = sqrtf(fmaxf(s2 / E - mu * mu, 0.0f));
+}
+
+#define MLP_TRY(expr)                                                                    \
+  do {                                                                                   \
+    cudaError_t e_ = (expr);                                                             \
+    if (e_ != cudaSuccess)                                                               \
+      return set_error(MCML_E_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+template <class T>
+void dfree(T *&p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+}  // namespace
+}  // namespace mcml
+
+using namespace mcml;
+
+struct mcml_mlp {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int in_dim = 0, in_pad = 0, hidden = 0, depth = 0, out_dim = 0, E = 0;
+  int layers = 0;                  // depth + 1 weight matrices
+  std::vector<int> fan_in, fan_out;
+  std::vector<long long> w_off, b_off;  // offsets into the per-member parameter block
+  long long per_member = 0;        // parameters per member
+  float *d_w = nullptr;            // E x per_member FP32 master (weights then biases per layer)
+  float *d_m = nullptr, *d_v = nullptr, *d_g = nullptr;
+  bf16 *d_w16 = nullptr;           // BF16 mirror (same layout)
+  float *d_xmean = nullptr, *d_xinv = nullptr, *d_tmean = nullptr, *d_tinv = nullptr,
+        *d_tstd = nullptr;
+  std::vector<float> h_tmean, h_tstd;
+  long long adam_t = 0;
+  // activations for a batch of up to cap rows
+  int cap = 0;
+  bf16 *d_x = nullptr;             // E x cap x in_pad
+  float *d_z = nullptr;            // E x depth x cap x hidden (pre-activations)
+  bf16 *d_h = nullptr;             // E x depth x cap x hidden (activations)
+  float *d_y = nullptr;            // E x cap x out
+  bf16 *d_dy = nullptr;            // E x cap x max(hidden, out)
+  bf16 *d_dh = nullptr;            // E x cap x hidden
+  uint32_t *d_idx = nullptr;       // E x cap
+  float *d_loss = nullptr;         // E
+
+  ~mcml_mlp() {
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != device) cudaSetDevice(device);
+    if (stream) cudaStreamSynchronize(stream);
+    dfree(d_w); dfree(d_m); dfree(d_v); dfree(d_g); dfree(d_w16);
+    dfree(d_xmean); dfree(d_xinv); dfree(d_tmean); dfree(d_tinv); dfree(d_tstd);
+    dfree(d_x); dfree(d_z); dfree(d_h); dfree(d_y); dfree(d_dy); dfree(d_dh); dfree(d_idx);
+    dfree(d_loss);
+    if (own_stream && stream) cudaStreamDestroy(stream);
+    if (prev >= 0 && prev != device) cudaSetDevice(prev);
+  }
+};
+
+namespace {
+
+struct MlpGuard {
+  int prev = -1;
+  bool changed = false;
+  explicit MlpGuard(int dev) {
+    if (cudaGetDevice(&prev) == cudaSuccess && prev != dev) changed = cudaSetDevice(dev) == cudaSuccess;
+  }
+  ~MlpGuard() {
+    if (changed) cudaSetDevice(prev);
+  }
+};
+
+int ensure_cap(mcml_mlp *p, int rows) {
+  if (rows <= p->cap) return MCML_OK;
+  dfree(p->d_x); dfree(p->d_z); dfree(p->d_h); dfree(p->d_y); dfree(p->d_dy); dfree(p->d_dh);
+  dfree(p->d_idx);
+  p->cap = 0;
+  const long long E = p->E, H = p->hidden, D = p->depth;
+  MLP_TRY(cudaMalloc(&p->d_x, E * rows * p->in_pad * sizeof(bf16)));
+  MLP_TRY(cudaMalloc(&p->d_z, E * D * rows * H * sizeof(float)));
+  MLP_TRY(cudaMalloc(&p->d_h, E * D * rows * H * sizeof(bf16)));
+  MLP_TRY(cudaMalloc(&p->d_y, E * rows * p->out_dim * sizeof(float)));
+  MLP_TRY(cudaMalloc(&p->d_dy, E * rows * std::max<long long>(H, p->out_dim) * sizeof(bf16)));
+  MLP_TRY(cudaMalloc(&p->d_dh, E * rows * H * sizeof(bf16)));
+  MLP_TRY(cudaMalloc(&p->d_idx, E * rows * sizeof(uint32_t)));
+  p->cap = rows;
+  return MCML_OK;
+}
+
+// Forward of all members on rows [0, n) already gathered into d_x.
+int forward(mcml_mlp *p, int n) {
+  const long long H = p->hidden, cap = p->cap, P = p->per_member;
+  for (int l = 0; l < p->layers; ++l) {
+    GemmArgs g;
+    std::memset(&g, 0, sizeof(g));
+    g.M = n;
+    g.N = p->fan_out[l];
+    g.K = l == 0 ? p->in_pad : (int)H;
+    if (l == 0) {
+      g.A = p->d_x;
+      g.lda = p->in_pad;
+      g.strideA = cap * p->in_pad;
+    } else {
+      g.A = p->d_h + (long long)(l - 1) * cap * H;
+      g.lda = H;
+      g.strideA = (long long)p->depth * cap * H;
+    }
+    g.B = p->d_w16 + p->w_off[l];
+    g.ldb = p->fan_out[l];
+    g.strideB = P;
+    g.bias = p->d_w + p->b_off[l];
+    g.strideBias = P;
+    if (l < p->depth) {
+      g.outF = p->d_z + (long long)l * cap * H;
+      g.ldo = H;
+      g.strideO = (long long)p->depth * cap * H;
+      g.outH = p->d_h + (long long)l * cap * H;
+      g.ldh = H;
+      g.strideH = (long long)p->depth * cap * H;
+      MLP_TRY((gemm<false, false, kBiasGelu>(g, p->E, p->stream)));
+    } else {
+      g.outF = p->d_y;
+      g.ldo = p->out_dim;
+      g.strideO = cap * p->out_dim;
+      MLP_TRY((gemm<false, false, kBias>(g, p->E, p->stream)));
+    }
+  }
+  return MCML_OK;
+}
+
+// Backward from dY (in d_dy, BF16) to all weight/bias gradients in d_g.
+int backward(mcml_mlp *p, int n) {
+  const long long H = p->hidden, cap = p->cap, P = p->per_member, D = p->depth;
+  bf16 *dcur = p->d_dy;   // gradient w.r.t. the current layer's output (pre-activation)
+  bf16 *dnext = p->d_dh;
+  long long dcur_ld = p->out_dim;
+  for (int l = p->layers - 1; l >= 0; --l) {
+    const int fo = p->fan_out[l], fi = p->fan_in[l];
+    // dW_l = X_l^T dZ_l  (M = fi, N = fo, K = n)
+    GemmArgs g;
+    std::memset(&g, 0, sizeof(g));
+    g.M = fi;
+    g.N = fo;
+    g.K = n;
+    if (l == 0) {
+      g.A = p->d_x;
+      g.lda = p->in_pad;
+      g.strideA = cap * p->in_pad;
+    } else {
+      g.A = p->d_h + (long long)(l - 1) * cap * H;
+      g.lda = H;
+      g.strideA = D * cap * H;
+    }
+    g.B = dcur;
+    g.ldb = dcur_ld;
+    g.strideB = cap * std::max<long long>(H, p->out_dim);
+    g.outF = p->d_g + p->w_off[l];
+    g.ldo = fo;
+    g.strideO = P;
+    MLP_TRY((gemm<true, false, kStoreF32>(g, p->E, p->stream)));
+    // db_l = column sums of dZ_l
+    bias_grad_kernel<<<dim3((fo + 127) / 128, 1, p->E), 128, 0, p->stream>>>(
+        dcur, cap * std::max<long long>(H, p->out_dim), n, fo, p->d_g + p->b_off[l], P);
+    MLP_TRY(cudaGetLastError());
+    if (l == 0) break;
+    // dZ_{l-1} = (dZ_l W_l^T) * gelu'(Z_{l-1})   (M = n, N = fi, K = fo)
+    GemmArgs b;
+    std::memset(&b, 0, sizeof(b));
+    b.M = n;
+    b.N = fi;
+    b.K = fo;
+    b.A = dcur;
+    b.lda = dcur_ld;
+    b.strideA = cap * std::max<long long>(H, p->out_dim);
+    b.B = p->d_w16 + p->w_off[l];
+    b.ldb = fo;
+    b.strideB = P;
+    b.outH = dnext;
+    b.ldh = H;
+    b.strideH = cap * std::max<long long>(H, p->out_dim);
+    b.aux = p->d_z + (long long)(l - 1) * cap * H;
+    b.ldx = H;
+    b.strideX = D * cap * H;
+    MLP_TRY((gemm<false, true, kGeluBack>(b, p->E, p->stream)));
+    std::swap(dcur, dnext);
+    dcur_ld = H;
+  }
+  return MCML_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mcml_mlp_create(const mcml_mlp_config *cfg, mcml_mlp **out) {
+  clear_error();
+  if (!cfg || !out) return set_error(MCML_E_INVALID, "mcml_mlp_create: null argument");
+  *out = nullptr;
+  if (cfg->in_dim < 1 || cfg->hidden < 16 || cfg->depth < 1 || cfg->out_dim < 1 ||
+      cfg->ensemble < 1 || cfg->in_dim > 4096 || cfg->hidden > 4096 ||
+      cfg->out_dim > cfg->hidden)
+    return set_error(MCML_E_INVALID, "mcml_mlp_create: bad dimensions");
+  std::unique_ptr<mcml_mlp> p(new mcml_mlp());
+  p->device = cfg->device;
+  MlpGuard gd(cfg->device);
+  p->in_dim = cfg->in_dim;
+  p->in_pad = (cfg->in_dim + 7) / 8 * 8;
+  p->hidden = cfg->hidden;
+  p->depth = cfg->depth;
+  p->out_dim = cfg->out_dim;
+  p->E = cfg->ensemble;
+  p->layers = cfg->depth + 1;
+  long long off = 0;
+  for (int l = 0; l < p->layers; ++l) {
+    const int fi = l == 0 ? p->in_pad : p->hidden;
+    const int fo = l == p->depth ? p->out_dim : p->hidden;
+    p->fan_in.push_back(fi);
+    p->fan_out.push_back(fo);
+    p->w_off.push_back(off);
+    off += (long long)fi * fo;
+    p->b_off.push_back(off);
+    off += fo;
+  }
+  p->per_member = off;
+  const long long total = off * p->E;
+  if (cfg->stream) {
+    p->stream = (cudaStream_t)cfg->stream;
+  } else {
+    MLP_TRY(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
+    p->own_stream = true;
+  }
+  MLP_TRY(cudaMalloc(&p->d_w, total * sizeof(float)));
+  MLP_TRY(cudaMalloc(&p->d_m, total * sizeof(float)));
+  MLP_TRY(cudaMalloc(&p->d_v, total * sizeof(float)));
+  MLP_TRY(cudaMalloc(&p->d_g, total * sizeof(float)));
+  MLP_TRY(cudaMalloc(&p->d_w16, total * sizeof(bf16)));
+  MLP_TRY(cudaMalloc(&p->d_xmean, p->in_pad * sizeof(float)));
+  MLP_TRY(cudaMalloc(&p->d_xinv, p->in_pad * sizeof(float)));
+  MLP_TRY(cudaMalloc(&p->d_tmean, p->out_dim * sizeof(float)));
+  MLP_TRY(cudaMalloc(&p->d_tinv, p->out_dim * sizeof(float)));
+  MLP_TRY(cudaMalloc(&p->d_tstd, p->out_dim * sizeof(float)));
+  MLP_TRY(cudaMalloc(&p->d_loss, p->E * sizeof(float)));
+  // He-uniform weights (per member seed), zero biases; the padded input
+  // rows of the first matrix are zero.
+  std::vector<float> w(total, 0.0f);
+  for (int e = 0; e < p->E; ++e) {
+    std::mt19937_64 rng(cfg->seed * 1000003ull + (uint64_t)e);
+    for (int l = 0; l < p->layers; ++l) {
+      const int fi = p->fan_in[l], fo = p->fan_out[l];
+      const int real_in = l == 0 ? p->in_dim : fi;
+      const float lim = std::sqrt(6.0f / (float)real_in) * (l == p->depth ? 0.5f : 1.0f);
+      std::uniform_real_distribution<float> U(-lim, lim);
+      float *W = w.data() + (long long)e * p->per_member + p->w_off[l];
+      for (int i = 0; i < fi; ++i)
+        for (int j = 0; j < fo; ++j) W[(long long)i * fo + j] = i < real_in ? U(rng) : 0.0f;
+    }
+  }
+  MLP_TRY(cudaMemcpy(p->d_w, w.data(), total * sizeof(float), cudaMemcpyHostToDevice));
+  MLP_TRY(cudaMemset(p->d_m, 0, total * sizeof(float)));
+  MLP_TRY(cudaMemset(p->d_v, 0, total * sizeof(float)));
+  to_bf16_kernel<<<(unsigned)((total + 255) / 256), 256, 0, p->stream>>>(p->d_w, p->d_w16, total);
+  MLP_TRY(cudaGetLastError());
+  std::vector<float> zeros(p->in_pad, 0.0f), ones(p->in_pad, 1.0f);
+  MLP_TRY(cudaMemcpy(p->d_xmean, zeros.data(), p->in_pad * sizeof(float), cudaMemcpyHostToDevice));
+  MLP_TRY(cudaMemcpy(p->d_xinv, ones.data(), p->in_pad * sizeof(float), cudaMemcpyHostToDevice));
+  p->h_tmean.assign(p->out_dim, 0.0f);
+  p->h_tstd.assign(p->out_dim, 1.0f);
+  MLP_TRY(cudaMemcpy(p->d_tmean, p->h_tmean.data(), p->out_dim * sizeof(float), cudaMemcpyHostToDevice));
+  MLP_TRY(cudaMemcpy(p->d_tinv, p->h_tstd.data(), p->out_dim * sizeof(float), cudaMemcpyHostToDevice));
+  MLP_TRY(cudaMemcpy(p->d_tstd, p->h_tstd.data(), p->out_dim * sizeof(float), cudaMemcpyHostToDevice));
+  MLP_TRY(cudaStreamSynchronize(p->stream));
+  *out = p.release();
+  return MCML_OK;
+}
+
+int mcml_mlp_set_normalization(mcml_mlp *p, const float *x_mean, const float *x_std,
+                               const float *t_mean, const float *t_std) {
+  clear_error();
+  if (!p || !x_mean || !x_std || !t_mean || !t_std) return set_error(MCML_E_INVALID, "null argument");
+  MlpGuard gd(p->device);
+  std::vector<float> xm(p->in_pad, 0.0f), xi(p->in_pad, 0.0f), tm(p->out_dim), ti(p->out_dim),
+      ts(p->out_dim);
+  for (int i = 0; i < p->in_dim; ++i) {
+    xm[i] = x_mean[i];
+    xi[i] = x_std[i] > 0 ? 1.0f / x_std[i] : 0.0f;  // a constant feature contributes nothing
+  }
+  for (int j = 0; j < p->out_dim; ++j) {
+    tm[j] = t_mean[j];
+    ts[j] = t_std[j] > 0 ? t_std[j] : 1.0f;
+    ti[j] = 1.0f / ts[j];
+  }
+  p->h_tmean = tm;
+  p->h_tstd = ts;
+  MLP_TRY(cudaMemcpy(p->d_xmean, xm.data(), p->in_pad * sizeof(float), cudaMemcpyHostToDevice));
+  MLP_TRY(cudaMemcpy(p->d_xinv, xi.data(), p->in_pad * sizeof(float), cudaMemcpyHostToDevice));
+  MLP_TRY(cudaMemcpy(p->d_tmean, tm.data(), p->out_dim * sizeof(float), cudaMemcpyHostToDevice));
+  MLP_TRY(cudaMemcpy(p->d_tinv, ti.data(), p->out_dim * sizeof(float), cudaMemcpyHostToDevice));
+  MLP_TRY(cudaMemcpy(p->d_tstd, ts.data(), p->out_dim * sizeof(float), cudaMemcpyHostToDevice));
+  return MCML_OK;
+}
+
+int64_t mcml_mlp_num_params(const mcml_mlp *p) { return p ? p->per_member : -1; }
+
+int mcml_mlp_get_params(mcml_mlp *p, float *host, int member) {
+  clear_error();
+  if (!p || !host || member < 0 || member >= p->E) return set_error(MCML_E_INVALID, "bad argument");
+  MlpGuard gd(p->device);
+  MLP_TRY(cudaStreamSynchronize(p->stream));
+  MLP_TRY(cudaMemcpy(host, p->d_w + (long long)member * p->per_member, p->per_member * sizeof(float),
+                     cudaMemcpyDeviceToHost));
+  return MCML_OK;
+}
+
+int mcml_mlp_set_params(mcml_mlp *p, const float *host, int member) {
+  clear_error();
+  if (!p || !host || member < 0 || member >= p->E) return set_error(MCML_E_INVALID, "bad argument");
+  MlpGuard gd(p->device);
+  float *dst = p->d_w + (long long)member * p->per_member;
+  MLP_TRY(cudaMemcpy(dst, host, p->per_member * sizeof(float), cudaMemcpyHostToDevice));
+  to_bf16_kernel<<<(unsigned)((p->per_member + 255) / 256), 256, 0, p->stream>>>(
+      dst, p->d_w16 + (long long)member * p->per_member, p->per_member);
+  MLP_TRY(cudaGetLastError());
+  MLP_TRY(cudaStreamSynchronize(p->stream));
+  return MCML_OK;
+}
+
+// One forward + backward on rows [0, n) of (X, T) for every member (no
+// update): loss per member and the FP32 gradients (host, E x num_params).
+int mcml_mlp_gradients(mcml_mlp *p, const float *X, const float *T, int n, float *loss_out,
+                       float *grads_out) {
+  clear_error();
+  if (!p || !X || !T || n < 1) return set_error(MCML_E_INVALID, "bad argument");
+  MlpGuard gd(p->device);
+  int rc = ensure_cap(p, n);
+  if (rc) return rc;
+  std::vector<uint32_t> idx((size_t)p->E * p->cap, 0);
+  for (int e = 0; e < p->E; ++e)
+    for (int i = 0; i < n; ++i) idx[(size_t)e * p->cap + i] = (uint32_t)i;
+  MLP_TRY(cudaMemcpyAsync(p->d_idx, idx.data(), idx.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                          p->stream));
+  const long long cap = p->cap;
+  gather_x_kernel<<<dim3((unsigned)((n * p->in_pad + 255) / 256), 1, p->E), 256, 0, p->stream>>>(
+      X, p->d_idx, n, p->in_dim, p->in_pad, p->d_xmean, p->d_xinv, cap, p->d_x, cap * p->in_pad);
+  MLP_TRY(cudaGetLastError());
+  rc = forward(p, n);
+  if (rc) return rc;
+  MLP_TRY(cudaMemsetAsync(p->d_loss, 0, p->E * sizeof(float), p->stream));
+  loss_grad_kernel<<<dim3((unsigned)((n * p->out_dim + 255) / 256), 1, p->E), 256, 0, p->stream>>>(
+      p->d_y, cap * p->out_dim, T, p->d_idx, cap, n, p->out_dim, p->d_tmean, p->d_tinv, p->d_dy,
+      cap * std::max(p->hidden, p->out_dim), p->d_loss);
+  MLP_TRY(cudaGetLastError());
+  rc = backward(p, n);
+  if (rc) return rc;
+  MLP_TRY(cudaStreamSynchronize(p->stream));
+  if (loss_out) MLP_TRY(cudaMemcpy(loss_out, p->d_loss, p->E * sizeof(float), cudaMemcpyDeviceToHost));
+  if (grads_out)
+    MLP_TRY(cudaMemcpy(grads_out, p->d_g, (size_t)p->E * p->per_member * sizeof(float),
+                       cudaMemcpyDeviceToHost));
+  return MCML_OK;
+}
+
+// One epoch of minibatch Adam over n rows of (X [n x in], T [n x out]),
+// DEVICE arrays.  Each member sees its own shuffle.  loss_out: mean loss
+// per member over the epoch (host, E floats).
+int mcml_mlp_train_epoch(mcml_mlp *p, const float *X, const float *T, uint64_t n, uint32_t batch,
+                         float lr, uint64_t shuffle_seed, float *loss_out) {
+  clear_error();
+  if (!p || !X || !T || n < 1 || batch < 1) return set_error(MCML_E_INVALID, "bad argument");
+  MlpGuard gd(p->device);
+  int rc = ensure_cap(p, (int)batch);
+  if (rc) return rc;
+  const long long cap = p->cap;
+  std::vector<std::vector<uint32_t>> perm(p->E, std::vector<uint32_t>(n));
+  for (int e = 0; e < p->E; ++e) {
+    for (uint64_t i = 0; i < n; ++i) perm[e][i] = (uint32_t)i;
+    std::mt19937_64 rng(shuffle_seed * 7919ull + (uint64_t)e);
+    std::shuffle(perm[e].begin(), perm[e].end(), rng);
+  }
+  std::vector<uint32_t> idx((size_t)p->E * cap);
+  std::vector<double> loss_sum(p->E, 0.0);
+  std::vector<float> loss(p->E);
+  uint64_t steps = 0;
+  const long long total = p->per_member * p->E;
+  for (uint64_t b0 = 0; b0 + batch <= n || (b0 < n && steps == 0); b0 += batch) {
+    const int rows = (int)std::min<uint64_t>(batch, n - b0);
+    for (int e = 0; e < p->E; ++e)
+      std::memcpy(&idx[(size_t)e * cap], &perm[e][b0], rows * sizeof(uint32_t));
+    MLP_TRY(cudaMemcpyAsync(p->d_idx, idx.data(), idx.size() * sizeof(uint32_t),
+                            cudaMemcpyHostToDevice, p->stream));
+    gather_x_kernel<<<dim3((unsigned)((rows * p->in_pad + 255) / 256), 1, p->E), 256, 0, p->stream>>>(
+        X, p->d_idx, rows, p->in_dim, p->in_pad, p->d_xmean, p->d_xinv, cap, p->d_x, cap * p->in_pad);
+    MLP_TRY(cudaGetLastError());
+    rc = forward(p, rows);
+    if (rc) return rc;
+    MLP_TRY(cudaMemsetAsync(p->d_loss, 0, p->E * sizeof(float), p->stream));
+    loss_grad_kernel<<<dim3((unsigned)((rows * p->out_dim + 255) / 256), 1, p->E), 256, 0, p->stream>>>(
+        p->d_y, cap * p->out_dim, T, p->d_idx, cap, rows, p->out_dim, p->d_tmean, p->d_tinv,
+        p->d_dy, cap * std::max(p->hidden, p->out_dim), p->d_loss);
+    MLP_TRY(cudaGetLastError());
+    rc = backward(p, rows);
+    if (rc) return rc;
+    ++p->adam_t;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.0f - std::pow(b1, (float)p->adam_t), c2 = 1.0f - std::pow(b2, (float)p->adam_t);
+    adam_kernel<<<(unsigned)((total + 255) / 256), 256, 0, p->stream>>>(
+        p->d_w, p->d_g, p->d_m, p->d_v, p->d_w16, total, lr, b1, b2, 1e-8f, c1, c2);
+    MLP_TRY(cudaGetLastError());
+    MLP_TRY(cudaMemcpyAsync(loss.data(), p->d_loss, p->E * sizeof(float), cudaMemcpyDeviceToHost,
+                            p->stream));
+    MLP_TRY(cudaStreamSynchronize(p->stream));
+    for (int e = 0; e < p->E; ++e) loss_sum[e] += loss[e];
+    ++steps;
+    if (rows < (int)batch) break;
+  }
+  if (loss_out)
+    for (int e = 0; e < p->E; ++e) loss_out[e] = (float)(loss_sum[e] / (double)steps);
+  return MCML_OK;
+}
+
+// Inference: X [n x in] DEVICE -> mean [n x out] and ensemble spread
+// [n x out] (DEVICE, de-normalised), in chunks of the activation buffers.
+int mcml_mlp_predict(mcml_mlp *p, const float *X, uint64_t n, float *mean, float *spread,
+                     uint32_t chunk) {
+  clear_error();
+  if (!p || !X || !mean) return set_error(MCML_E_INVALID, "bad argument");
+  MlpGuard gd(p->device);
+  if (chunk == 0) chunk = 65536;
+  int rc = ensure_cap(p, (int)std::min<uint64_t>(chunk, n));
+  if (rc) return rc;
+  const long long cap = p->cap;
+  for (uint64_t r0 = 0; r0 < n; r0 += cap) {
+    const int rows = (int)std::min<uint64_t>(cap, n - r0);
+    gather_x_kernel<<<dim3((unsigned)((rows * p->in_pad + 255) / 256), 1, p->E), 256, 0, p->stream>>>(
+        X + r0 * p->in_dim, nullptr, rows, p->in_dim, p->in_pad, p->d_xmean, p->d_xinv, 0, p->d_x,
+        cap * p->in_pad);
+    MLP_TRY(cudaGetLastError());
+    rc = forward(p, rows);
+    if (rc) return rc;
+    ensemble_kernel<<<(unsigned)(((long long)rows * p->out_dim + 255) / 256), 256, 0, p->stream>>>(
+        p->d_y, cap * p->out_dim, p->E, (long long)rows * p->out_dim, p->d_tmean, p->d_tstd,
+        p->out_dim, mean + r0 * p->out_dim, spread ? spread + r0 * p->out_dim : nullptr);
+    MLP_TRY(cudaGetLastError());
+  }
+  return MCML_OK;
+}
+
+int mcml_mlp_sync(mcml_mlp *p) {
+  clear_error();
+  if (!p) return set_error(MCML_E_INVALID, "null mlp");
+  MlpGuard gd(p->device);
+  MLP_TRY(cudaStreamSynchronize(p->stream));
+  return MCML_OK;
+}
+
+void mcml_mlp_destroy(mcml_mlp *p) { delete p; }
+
+}  // extern "C"

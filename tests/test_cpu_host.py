@@ -32,8 +32,8 @@ def test_library_exports_every_declared_entry_point():
     for n in names:
         assert hasattr(lib, n), n
     # the Python bindings cover the whole header
-    from mcml_gpu_b200 import wmc
-    assert set(names) == set(m.exported_symbols()) | set(wmc.BOUND)
+    from mcml_gpu_b200 import surrogate, wmc
+    assert set(names) == set(m.exported_symbols()) | set(wmc.BOUND) | set(surrogate.BOUND)
 
 
 def test_version_and_strerror():
