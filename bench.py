@@ -277,6 +277,104 @@ def batch_arm(args) -> int:
     return 0
 
 
+def surrogate_arm(args) -> int:
+    """Configs 3-4: White-MC labels from replayed baselines of the 5-layer
+    tissue (ring detectors at 0.5/1.0/1.5 cm, tests/golden/configs/surrogate),
+    ensemble training on the GPU, serving of 1e6 queries (5 % outside the
+    training hull, whose answers come from plain MC at 1e7 photons), and the
+    error against plain MC on held-out tissues."""
+    import torch
+    import mcml_gpu_b200 as m
+    import mcml_gpu_b200.surrogate as sg
+    cfg = ROOT / "tests" / "golden" / "configs" / "surrogate"
+    base = m.parse_config(cfg / "sim_set.json", cfg / "input.txt")[0]
+    L = int(base.num_layers)
+    t0 = time.perf_counter()
+    labels = sg.make_labels(base, n_baselines=args.baselines, photons=int(args.label_photons),
+                            combos_per_baseline=args.combos // args.baselines, seed=1)
+    label_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    sur = sg.Surrogate.train(labels, epochs=args.epochs, batch=4096, lr=2e-3, seed=1,
+                             max_spread=0.05, fallback_photons=10_000_000)
+    train_s = time.perf_counter() - t0
+    rng = np.random.default_rng(5)
+    # 1e6 queries: 95 % drawn like the labels, 5 % with mua widened 20 % past its range
+    nq = args.queries
+    bidx = rng.integers(0, len(labels.baselines), nq)
+    X = np.repeat(sg.features(labels.baselines[:1]), nq, axis=0)
+    mus_b = np.array([[b.mus[l] for l in range(L)] for b in labels.baselines])
+    for l in range(L):
+        X[:, 5 * l + 1] = rng.uniform(0.05, 0.5, nq)
+        X[:, 5 * l + 2] = mus_b[bidx, l] * rng.uniform(0.95, 1.05, nq)
+    out = rng.random(nq) < 0.05
+    X[out, 1] = rng.uniform(0.5, 0.59, out.sum())
+    Xt = torch.from_numpy(X).cuda()
+    sur.mlp.predict(Xt[:65536])  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    mean, spread = sur.mlp.predict(Xt)
+    torch.cuda.synchronize()
+    mlp_s = time.perf_counter() - t0
+    inside = np.all((X >= sur.lo - 1e-6) & (X <= sur.hi + 1e-6), axis=1)
+    agree = np.all(spread.cpu().numpy() <= sur.max_spread, axis=1)
+    fallback = ~(inside & agree)
+    # cost of the fallback: plain MC at 1e7 photons for a sample of flagged queries
+    fb_idx = np.nonzero(fallback)[0][:16]
+    fb = []
+    for i in fb_idx:
+        s = m.Sim.from_buffer_copy(labels.baselines[0])
+        for l in range(L):
+            s.mua[l], s.mus[l] = float(X[i, 5 * l + 1]), float(X[i, 5 * l + 2])
+        s.number_photons = 10_000_000
+        fb.append(s)
+    with m.Batch(fb, seed=3) as b:
+        b.run()
+        res = b.run()
+    fb_per_query_s = res[0].walk_ms / 1e3 / max(len(fb), 1)
+    serve_s = mlp_s + fallback.sum() * fb_per_query_s
+    # error against plain MC on held-out tissues (drawn like the labels)
+    held = []
+    for k in range(args.heldout):
+        b = labels.baselines[k % len(labels.baselines)]
+        s = m.Sim.from_buffer_copy(b)
+        for l in range(L):
+            s.mua[l] = float(rng.uniform(0.05, 0.5))
+            s.mus[l] = float(b.mus[l] * rng.uniform(0.95, 1.05))
+        s.number_photons = int(args.ref_photons)
+        held.append(s)
+    with m.Batch(held, seed=11) as b:
+        ref = b.run()
+    mc_rate = sum(int(s.number_photons) for s in held) / (ref[0].walk_ms / 1e3)
+    R_ref = np.array([r.reflectance[:3] for r in ref])
+    se = np.array([r.std_error[:3] for r in ref]) / R_ref
+    logR, _ = sur.predict(sg.features(held))
+    rel = np.abs(np.exp(logR) - R_ref) / R_ref
+    mc_evals = mc_rate / float(args.ref_photons)
+    print(json.dumps({
+        "metric": "SDS-reflectance evals/s", "impl": "mcml-surrogate",
+        "value": nq / serve_s, "unit": "evals/s",
+        "mlp_only_evals_per_s": nq / mlp_s,
+        "plain_mc_evals_per_s_at_ref_photons": mc_evals,
+        "speedup_vs_plain_mc": (nq / serve_s) / mc_evals,
+        "speedup_vs_plain_mc_inside_hull": (nq / mlp_s) / mc_evals,
+        "fallback_fraction": float(fallback.mean()),
+        "fallback_s_per_query_at_1e7": fb_per_query_s,
+        "error_vs_plain_mc": {"median_rel": float(np.median(rel)),
+                              "p90_rel": float(np.percentile(rel, 90)),
+                              "per_sds_median": [float(v) for v in np.median(rel, axis=0)],
+                              "mc_rel_se_median": float(np.median(se)),
+                              "heldout": args.heldout, "ref_photons": int(args.ref_photons)},
+        "labels": {"count": int(labels.X.shape[0]), "baselines": args.baselines,
+                   "photons_per_baseline": int(args.label_photons), "seconds": label_s},
+        "training": {"epochs": args.epochs, "seconds": train_s,
+                     "final_loss": [float(v) for v in sur.history[-1]]},
+        "config": {"workload": "configs 3-4: WMC labels, MLP 25->256x4->3 GELU, ensemble 4, "
+                               "BF16 tensor-core kernels; ring detectors 0.5/1.0/1.5 cm",
+                   "queries": nq},
+    }), flush=True)
+    return 0
+
+
 def read_traffic(slots: int) -> float | None:
     """DRAM bytes of one walk launch: the ncu-measured bytes per slot of a
     smaller capture (profiles/walk_kernel_traffic.json) times this run's
@@ -433,8 +531,8 @@ def main() -> int:
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", choices=["mcml", "reference", "reference-gpu", "batch"],
-                    default="mcml")
+    ap.add_argument("--impl", default="mcml",
+                    choices=["mcml", "reference", "reference-gpu", "batch", "surrogate"])
     ap.add_argument("--photons", type=int, default=0, help="override N (default: 1e8)")
     ap.add_argument("--slots", type=int, default=0)
     ap.add_argument("--block", type=int, default=0)
@@ -446,6 +544,13 @@ def main() -> int:
     ap.add_argument("--sets", type=int, default=4096)
     ap.add_argument("--min-photons", type=float, default=1e5)
     ap.add_argument("--max-photons", type=float, default=1e7)
+    ap.add_argument("--baselines", type=int, default=64)
+    ap.add_argument("--label-photons", type=float, default=2e7)
+    ap.add_argument("--combos", type=int, default=2_000_000)
+    ap.add_argument("--epochs", type=int, default=12)
+    ap.add_argument("--queries", type=int, default=1_000_000)
+    ap.add_argument("--heldout", type=int, default=128)
+    ap.add_argument("--ref-photons", type=float, default=1e8)
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -453,6 +558,8 @@ def main() -> int:
         return reference_gpu_arm(args)
     if args.impl == "batch":
         return batch_arm(args)
+    if args.impl == "surrogate":
+        return surrogate_arm(args)
     return mcml_arm(args)
 
 
