@@ -277,6 +277,40 @@ def batch_arm(args) -> int:
     return 0
 
 
+def reference_plain_mc_evals(cfg: Path, sims, photons: int) -> float | None:
+    """Plain-MC evaluations per second of the reference's CUDA build
+    (oracle/_ref/MCML_GPU) on the same tissues: one multi-simulation run,
+    wall clock from process start to exit."""
+    import oracle
+    if not oracle.REF_BIN.exists():
+        return None
+    conf = json.loads((cfg / "sim_set.json").read_text())
+    conf["number_photons"] = photons
+    conf["number_simulation"] = len(sims)
+    lines = []
+    for s in sims:
+        L = int(s.num_layers)
+        vals = []
+        for l in range(L):
+            if l < L - 1:
+                vals.append(s.height[l])
+            vals += [s.mua[l], s.mus[l], s.n[l], s.g[l]]
+        lines.append("\t".join(f"{float(v):.9g}" for v in vals))
+    with tempfile.TemporaryDirectory() as td:
+        (Path(td) / "sim_set.json").write_text(json.dumps(conf))
+        (Path(td) / "input.txt").write_text("\n".join(lines) + "\n")
+        env = dict(os.environ, MCML_FIXED_TIME="1234", LD_PRELOAD=str(oracle.REF_SHIM))
+        t0 = time.perf_counter()
+        res = subprocess.run([str(oracle.REF_BIN), "sim_set.json", "input.txt", "output.txt"],
+                             cwd=td, env=env, capture_output=True, text=True, timeout=3600)
+        dt = time.perf_counter() - t0
+    return len(sims) / dt if res.returncode == 0 else None
+
+
+MUA_RANGE = (0.05, 0.5)   # 1/cm, config 1
+MUS_RANGE = (50.0, 250.0)  # 1/cm, config 1
+
+
 def surrogate_arm(args) -> int:
     """Configs 3-4: White-MC labels from replayed baselines of the 5-layer
     tissue (ring detectors at 0.5/1.0/1.5 cm, tests/golden/configs/surrogate),
@@ -291,23 +325,29 @@ def surrogate_arm(args) -> int:
     L = int(base.num_layers)
     t0 = time.perf_counter()
     labels = sg.make_labels(base, n_baselines=args.baselines, photons=int(args.label_photons),
-                            combos_per_baseline=args.combos // args.baselines, seed=1)
+                            combos_per_baseline=args.combos // args.baselines, seed=1,
+                            mua_range=MUA_RANGE, mus_range=MUS_RANGE)
     label_s = time.perf_counter() - t0
     t0 = time.perf_counter()
     sur = sg.Surrogate.train(labels, epochs=args.epochs, batch=4096, lr=2e-3, seed=1,
                              max_spread=0.05, fallback_photons=10_000_000)
     train_s = time.perf_counter() - t0
     rng = np.random.default_rng(5)
-    # 1e6 queries: 95 % drawn like the labels, 5 % with mua widened 20 % past its range
+    # 1e6 queries: mua and mus of every layer uniform over config 1's ranges;
+    # 5 % of them take one coefficient from the 20 %-widened ranges' excess,
+    # outside the training hull
     nq = args.queries
-    bidx = rng.integers(0, len(labels.baselines), nq)
     X = np.repeat(sg.features(labels.baselines[:1]), nq, axis=0)
-    mus_b = np.array([[b.mus[l] for l in range(L)] for b in labels.baselines])
     for l in range(L):
-        X[:, 5 * l + 1] = rng.uniform(0.05, 0.5, nq)
-        X[:, 5 * l + 2] = mus_b[bidx, l] * rng.uniform(0.95, 1.05, nq)
+        X[:, 5 * l + 1] = rng.uniform(*MUA_RANGE, nq)
+        X[:, 5 * l + 2] = rng.uniform(*MUS_RANGE, nq)
     out = rng.random(nq) < 0.05
-    X[out, 1] = rng.uniform(0.5, 0.59, out.sum())
+    for i in np.nonzero(out)[0]:
+        l, which = rng.integers(0, L), rng.integers(1, 3)
+        lo, hi = MUA_RANGE if which == 1 else MUS_RANGE
+        ext = 0.2 * (hi - lo)
+        X[i, 5 * l + which] = (rng.uniform(lo - ext, lo) if rng.random() < 0.5
+                               else rng.uniform(hi, hi + ext))
     Xt = torch.from_numpy(X).cuda()
     sur.mlp.predict(Xt[:65536])  # warm-up
     torch.cuda.synchronize()
@@ -333,13 +373,13 @@ def surrogate_arm(args) -> int:
     fb_per_query_s = res[0].walk_ms / 1e3 / max(len(fb), 1)
     serve_s = mlp_s + fallback.sum() * fb_per_query_s
     # error against plain MC on held-out tissues (drawn like the labels)
+    # held-out tissues drawn like the in-hull queries
     held = []
     for k in range(args.heldout):
-        b = labels.baselines[k % len(labels.baselines)]
-        s = m.Sim.from_buffer_copy(b)
+        s = m.Sim.from_buffer_copy(labels.baselines[0])
         for l in range(L):
-            s.mua[l] = float(rng.uniform(0.05, 0.5))
-            s.mus[l] = float(b.mus[l] * rng.uniform(0.95, 1.05))
+            s.mua[l] = float(rng.uniform(*MUA_RANGE))
+            s.mus[l] = float(rng.uniform(*MUS_RANGE))
         s.number_photons = int(args.ref_photons)
         held.append(s)
     with m.Batch(held, seed=11) as b:
@@ -350,6 +390,7 @@ def surrogate_arm(args) -> int:
     logR, _ = sur.predict(sg.features(held))
     rel = np.abs(np.exp(logR) - R_ref) / R_ref
     mc_evals = mc_rate / float(args.ref_photons)
+    ref_evals = reference_plain_mc_evals(cfg, held[:2], int(args.ref_photons))
     print(json.dumps({
         "metric": "SDS-reflectance evals/s", "impl": "mcml-surrogate",
         "value": nq / serve_s, "unit": "evals/s",
@@ -357,6 +398,8 @@ def surrogate_arm(args) -> int:
         "plain_mc_evals_per_s_at_ref_photons": mc_evals,
         "speedup_vs_plain_mc": (nq / serve_s) / mc_evals,
         "speedup_vs_plain_mc_inside_hull": (nq / mlp_s) / mc_evals,
+        "reference_plain_mc_evals_per_s": ref_evals,
+        "speedup_vs_reference_plain_mc": (nq / serve_s) / ref_evals if ref_evals else None,
         "fallback_fraction": float(fallback.mean()),
         "fallback_s_per_query_at_1e7": fb_per_query_s,
         "error_vs_plain_mc": {"median_rel": float(np.median(rel)),
@@ -544,12 +587,12 @@ def main() -> int:
     ap.add_argument("--sets", type=int, default=4096)
     ap.add_argument("--min-photons", type=float, default=1e5)
     ap.add_argument("--max-photons", type=float, default=1e7)
-    ap.add_argument("--baselines", type=int, default=64)
-    ap.add_argument("--label-photons", type=float, default=2e7)
+    ap.add_argument("--baselines", type=int, default=512)
+    ap.add_argument("--label-photons", type=float, default=2.5e6)
     ap.add_argument("--combos", type=int, default=2_000_000)
     ap.add_argument("--epochs", type=int, default=12)
     ap.add_argument("--queries", type=int, default=1_000_000)
-    ap.add_argument("--heldout", type=int, default=128)
+    ap.add_argument("--heldout", type=int, default=1000)
     ap.add_argument("--ref-photons", type=float, default=1e8)
     args = ap.parse_args()
     if args.impl == "reference":

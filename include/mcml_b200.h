@@ -40,6 +40,7 @@ extern "C" {
 
 typedef enum mcml_status {
   MCML_OK = 0,
+  MCML_INCOMPLETE = 1,  /* a checkpointed run stopped early; call again */
   MCML_E_INVALID = -1,  /* bad argument or configuration value        */
   MCML_E_CUDA = -2,     /* a CUDA runtime call failed                  */
   MCML_E_NOMEM = -3,    /* host or device allocation failed            */
@@ -48,7 +49,8 @@ typedef enum mcml_status {
   MCML_E_PARSE = -6,    /* sim_set.json / input.txt could not be read  */
   MCML_E_STATE = -7,    /* calls made in the wrong order               */
   MCML_E_BUDGET = -8,   /* a kernel hit its step budget and stopped    */
-  MCML_E_NODEV = -9     /* no CUDA device                              */
+  MCML_E_NODEV = -9,    /* no CUDA device                              */
+  MCML_E_CHECKPOINT = -10 /* checkpoint file corrupt or of another run  */
 } mcml_status;
 
 /*
@@ -375,6 +377,51 @@ typedef struct mcml_noalloc_result {
 } mcml_noalloc_result;
 int mcml_run_noalloc(const mcml_sim *sim, uint64_t seed, uint64_t slots, int device,
                      void *stream, mcml_noalloc_result *out);
+
+/* ---- checkpoint / resume of the first pass ----------------------------- */
+/*
+ * The first pass walked in launches of chunk_slots slots, with a
+ * checkpoint file brought up to date after every launch -- the launch
+ * boundary of the reference's host loop (transport.cu:114-150), where its
+ * thread states, quotas and counters come back to the host.  Here a slot's
+ * photons depend only on (seed, slot), so the checkpoint holds the slot
+ * range done, the step count and the detection records so far; the slot
+ * states are re-seeded.  If `path` exists, the run resumes after its last
+ * completed launch; it must belong to the same simulation, seed,
+ * slot_begin and slot count (else MCML_E_CHECKPOINT, the file untouched).
+ * A resumed run detects the same photons as one uninterrupted mcml_run
+ * with the same seed and slots; mcml_replay and the getters then work as
+ * after mcml_run.  The file is append-only: records of a launch are
+ * written and flushed before the header that counts them, so a crash
+ * during an update leaves the previous checkpoint readable.
+ *
+ * File layout (little-endian): a 128-byte header {char magic[8]
+ * "MCMLCKP1"; u32 version 1; u32 record_bytes 40; u64 run_digest, seed,
+ * slot_begin, photons, slots, slots_done, records, steps, launches,
+ * records_digest, header_digest; 24 zero bytes} followed by `records`
+ * detection records {u64 photon; u32 sds; f32 weight; u32 xorwow d,
+ * v[5]}.  Digests are 64-bit FNV-1a; header_digest covers the 96 bytes
+ * before it, records_digest the record bytes in file order.
+ */
+typedef struct mcml_checkpoint_opts {
+  const char *path;
+  uint64_t chunk_slots; /* slots per launch; 0 = the larger of 32 slots per
+                           resident thread and slots / 64                   */
+  uint32_t max_chunks;  /* return MCML_INCOMPLETE after this many launches in
+                           this call (0 = run to the end)                   */
+  uint32_t reserved;
+} mcml_checkpoint_opts;
+
+typedef struct mcml_checkpoint_info {
+  uint64_t seed, slot_begin, photons, slots;
+  uint64_t slots_done, records, steps, launches;
+} mcml_checkpoint_info;
+
+/* MCML_OK when every slot is walked (result filled as by mcml_run),
+ * MCML_INCOMPLETE when stopped by max_chunks (result untouched). */
+int mcml_run_checkpointed(mcml_ctx *ctx, const mcml_checkpoint_opts *ck, mcml_result *result);
+/* Reads and checks a checkpoint file on the host (no device needed). */
+int mcml_checkpoint_read_info(const char *path, mcml_checkpoint_info *info);
 
 /* ---- test support ------------------------------------------------------ */
 /*

@@ -23,7 +23,7 @@ __all__ = [
     "MAX_LAYERS", "MAX_SDS", "MCMLError", "Sim", "Opts", "Result", "Derived",
     "DeviceInfo", "load_library", "lib_path", "parse_config", "derive", "make_sim",
     "Simulation", "Batch", "sample_sets", "shard", "uniform_stream", "device_count",
-    "device_info",
+    "device_info", "checkpoint_info", "CheckpointInfo", "INCOMPLETE",
     "OUT_REPLAY", "OUT_ABSORBANCE", "OUT_PATHLENGTH", "OUT_AVERAGE_PL", "OUT_BINARY",
 ]
 
@@ -176,6 +176,22 @@ class BatchTuning(C.Structure):
     ]
 
 
+class CheckpointOpts(C.Structure):
+    _fields_ = [
+        ("path", C.c_char_p),
+        ("chunk_slots", C.c_uint64),
+        ("max_chunks", C.c_uint32),
+        ("reserved", C.c_uint32),
+    ]
+
+
+class CheckpointInfo(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in ("seed", "slot_begin", "photons", "slots", "slots_done",
+                                          "records", "steps", "launches")]
+
+
+INCOMPLETE = 1  # MCML_INCOMPLETE: a checkpointed run stopped early
+
 _lib: Optional[C.CDLL] = None
 
 # (name, restype, argtypes) of every entry point of include/mcml_b200.h
@@ -215,6 +231,9 @@ _SIGNATURES = [
     ("mcml_batch_launch", C.c_int, [C.c_void_p]),
     ("mcml_batch_get_results", C.c_int, [C.c_void_p, C.c_void_p]),
     ("mcml_batch_destroy", None, [C.c_void_p]),
+    ("mcml_run_checkpointed", C.c_int, [C.c_void_p, C.POINTER(CheckpointOpts),
+                                        C.POINTER(Result)]),
+    ("mcml_checkpoint_read_info", C.c_int, [C.c_char_p, C.POINTER(CheckpointInfo)]),
 ]
 
 
@@ -318,6 +337,15 @@ def shard(rank: int, world: int, photons: int, weak: bool = True) -> tuple[int, 
     return rank * base + min(rank, extra), n
 
 
+def checkpoint_info(path: os.PathLike | str) -> CheckpointInfo:
+    """Header of a checkpoint file, checked (no device needed)."""
+    lib = load_library()
+    info = CheckpointInfo()
+    _check(lib.mcml_checkpoint_read_info(os.fsencode(str(path)), C.byref(info)),
+           "mcml_checkpoint_read_info")
+    return info
+
+
 def uniform_stream(seed: int, subsequence: int, count: int, device: int = 0) -> np.ndarray:
     """The first `count` curand_uniform draws of XORWOW subsequence
     `subsequence` under `seed` (the stream of the reference's thread)."""
@@ -374,6 +402,19 @@ class Simulation:
     def run(self) -> Result:
         r = Result()
         _check(self._lib.mcml_run(self._ctx, C.byref(r)), "mcml_run")
+        return r
+
+    def run_checkpointed(self, path: os.PathLike | str, *, chunk_slots: int = 0,
+                         max_chunks: int = 0) -> Optional[Result]:
+        """First pass in launches of chunk_slots slots, checkpointed to
+        `path` after each (resuming from it if present).  Returns the
+        result, or None when max_chunks launches ran and slots remain."""
+        o = CheckpointOpts(os.fsencode(str(path)), int(chunk_slots), int(max_chunks), 0)
+        r = Result()
+        rc = self._lib.mcml_run_checkpointed(self._ctx, C.byref(o), C.byref(r))
+        if rc == INCOMPLETE:
+            return None
+        _check(rc, "mcml_run_checkpointed")
         return r
 
     def launch_run(self) -> None:

@@ -191,9 +191,15 @@ int ensure_records(mcml_ctx *c, uint64_t cap) {
   return MCML_OK;
 }
 
+// -1 when either event was never recorded; the failed query's error is
+// taken off the thread's last-error slot so a later launch check does not
+// report it.
 float elapsed(cudaEvent_t a, cudaEvent_t b) {
   float ms = 0.0f;
-  if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) ms = -1.0f;
+  if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) {
+    cudaGetLastError();
+    ms = -1.0f;
+  }
   return ms;
 }
 
@@ -286,6 +292,7 @@ int launch_run(mcml_ctx *c) {
   A.counters = c->d_counters;
   A.records = c->d_records;
   A.rec_cap = c->rec_cap;
+  A.slot_end = c->S;
   CUDA_TRY(launch_walk(c->P, A, c->sim.source_probe_oblique != 0,
                        c->sim.detector_probe_oblique != 0, c->walk_block, c->walk_min_blocks,
                        c->walk_grid, c->stream));
@@ -567,6 +574,128 @@ int mcml_run(mcml_ctx *ctx, mcml_result *result) {
     rc = fill_result(ctx, result);
   }
   return rc;
+}
+
+int mcml_run_checkpointed(mcml_ctx *c, const mcml_checkpoint_opts *ck, mcml_result *result) {
+  clear_error();
+  if (!c || !ck || !ck->path || !ck->path[0]) return set_error(MCML_E_INVALID, "null argument");
+  DeviceGuard g(c->device);
+  const std::string path = ck->path;
+  const uint64_t digest = run_digest(c->sim, c->opts.seed, c->opts.slot_begin, c->S);
+  CkptHeader h;
+  bool exists = false;
+  int rc = ckpt_read_header(path, h, exists);
+  if (rc) return rc;
+  if (exists) {
+    if (h.run_digest != digest || h.seed != c->opts.seed || h.slot_begin != c->opts.slot_begin ||
+        h.photons != c->N || h.slots != c->S)
+      return set_error(MCML_E_CHECKPOINT, "checkpoint " + path +
+                                              " belongs to another simulation, seed or slot layout");
+  } else {
+    ckpt_init(h);
+    h.run_digest = digest;
+    h.seed = c->opts.seed;
+    h.slot_begin = c->opts.slot_begin;
+    h.photons = c->N;
+    h.slots = c->S;
+    rc = ckpt_write_header(path, h);
+    if (rc) return rc;
+  }
+  c->ran = c->replayed = c->host_valid = false;
+
+  // Records so far back onto the device.
+  uint64_t D = h.records;
+  if (D > c->rec_cap) {
+    rc = ensure_records(c, D + D / 4 + 1024);
+    if (rc) return rc;
+  }
+  if (D) {
+    std::vector<DetRecord> host(D);
+    rc = ckpt_read_records(path, h, host.data());
+    if (rc) return rc;
+    CUDA_TRY(cudaMemcpy(c->d_records, host.data(), D * sizeof(DetRecord), cudaMemcpyHostToDevice));
+  }
+  CUDA_TRY(cudaMemsetAsync(c->d_sums, 0, 96 * sizeof(unsigned long long), c->stream));
+  CUDA_TRY(cudaEventRecord(c->ev[0], c->stream));
+  CUDA_TRY(launch_seed_slots(c->opts.seed, c->opts.slot_begin, c->S, c->d_slot_state,
+                             c->sm_count, c->stream));
+  CUDA_TRY(cudaEventRecord(c->ev[2], c->stream));
+
+  const uint64_t lanes = (uint64_t)c->walk_grid * (uint64_t)c->walk_block;
+  uint64_t chunk = ck->chunk_slots ? ck->chunk_slots : std::max<uint64_t>(32 * lanes, c->S / 64);
+  chunk = std::max<uint64_t>(1, std::min<uint64_t>(chunk, c->S));
+  uint64_t done = h.slots_done, steps = h.steps;
+  uint32_t launched = 0;
+  double walk_ms = 0.0;
+  std::vector<DetRecord> fresh;
+  while (done < c->S) {
+    if (ck->max_chunks && launched >= ck->max_chunks) return MCML_INCOMPLETE;
+    const uint64_t end = std::min<uint64_t>(c->S, done + chunk);
+    unsigned long long cnt[kCntWords] = {};
+    cnt[kCntSlot] = done;
+    cnt[kCntRecords] = D;
+    cnt[kCntSteps] = steps;
+    CUDA_TRY(cudaMemcpyAsync(c->d_counters, cnt, sizeof(cnt), cudaMemcpyHostToDevice, c->stream));
+    WalkArgs A;
+    A.slot_state = c->d_slot_state;
+    A.counters = c->d_counters;
+    A.records = c->d_records;
+    A.rec_cap = c->rec_cap;
+    A.slot_end = end;
+    CUDA_TRY(cudaEventRecord(c->ev[4], c->stream));
+    CUDA_TRY(launch_walk(c->P, A, c->sim.source_probe_oblique != 0,
+                         c->sim.detector_probe_oblique != 0, c->walk_block, c->walk_min_blocks,
+                         c->walk_grid, c->stream));
+    CUDA_TRY(cudaEventRecord(c->ev[1], c->stream));
+    CUDA_TRY(cudaMemcpyAsync(cnt, c->d_counters, sizeof(cnt), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (cnt[kCntRecords] > c->rec_cap) {
+      // Records beyond the buffer were dropped: grow it, keep the first D,
+      // walk this launch's slots again (their photons do not change).
+      const uint64_t cap = cnt[kCntRecords] + cnt[kCntRecords] / 4 + 1024;
+      DetRecord *bigger = nullptr;
+      CUDA_TRY(cudaMalloc(&bigger, cap * sizeof(DetRecord)));
+      if (D)
+        CUDA_TRY(cudaMemcpy(bigger, c->d_records, D * sizeof(DetRecord), cudaMemcpyDeviceToDevice));
+      dfree(c->d_records);
+      c->d_records = bigger;
+      c->rec_cap = cap;
+      continue;
+    }
+    walk_ms += elapsed(c->ev[4], c->ev[1]);
+    const uint64_t n = cnt[kCntRecords] - D;
+    fresh.resize(n);
+    if (n)
+      CUDA_TRY(cudaMemcpy(fresh.data(), c->d_records + D, n * sizeof(DetRecord),
+                          cudaMemcpyDeviceToHost));
+    rc = ckpt_append(path, h, fresh.data(), n, end, cnt[kCntSteps]);
+    if (rc) return rc;
+    D = cnt[kCntRecords];
+    steps = cnt[kCntSteps];
+    done = end;
+    ++launched;
+  }
+  // All slots walked: the state mcml_run leaves behind.
+  {
+    unsigned long long cnt[kCntWords] = {};
+    cnt[kCntSlot] = c->S;
+    cnt[kCntRecords] = D;
+    cnt[kCntSteps] = steps;
+    CUDA_TRY(cudaMemcpyAsync(c->d_counters, cnt, sizeof(cnt), cudaMemcpyHostToDevice, c->stream));
+  }
+  CUDA_TRY(launch_reduce_records(c->d_records, c->d_counters + kCntRecords, c->rec_cap,
+                                 c->sim.num_sds, c->d_sums,
+                                 reinterpret_cast<double *>(c->d_sums + 32),
+                                 reinterpret_cast<double *>(c->d_sums + 64), c->sm_count,
+                                 c->stream));
+  c->ran = true;
+  rc = fill_result(c, result);
+  if (rc) return rc;
+  if (result) {
+    result->walk_ms = (float)walk_ms;
+    result->seed_ms = elapsed(c->ev[0], c->ev[2]);
+  }
+  return MCML_OK;
 }
 
 int mcml_launch_replay(mcml_ctx *ctx) {

@@ -1,6 +1,7 @@
 // internal.h -- helpers shared by the library's host translation units.
 #pragma once
 
+#include <cstddef>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -46,5 +47,35 @@ int write_pathlength(const HostOutputs &o, const std::string &dir, bool binary);
 int write_average_pathlength(const HostOutputs &o, const std::string &path);
 int write_A_rz(const HostOutputs &o, const std::string &dir, bool binary);
 int write_A0_z(const HostOutputs &o, const std::string &dir, bool binary);
+
+// Checkpoint file of a chunked first pass (checkpoint.cpp); the layout is
+// the one documented beside mcml_run_checkpointed.
+constexpr uint64_t kFnvBasis = 14695981039346656037ull;
+constexpr uint32_t kRecordBytes = 40;
+struct CkptHeader {
+  char magic[8];
+  uint32_t version;
+  uint32_t record_bytes;
+  uint64_t run_digest;
+  uint64_t seed, slot_begin, photons, slots;
+  uint64_t slots_done;
+  uint64_t records;
+  uint64_t steps;
+  uint64_t launches;
+  uint64_t records_digest;
+  uint64_t header_digest;
+  uint64_t zero[3];
+};
+uint64_t fnv1a(const void *p, size_t n, uint64_t h);
+uint64_t run_digest(const mcml_sim &s, uint64_t seed, uint64_t slot_begin, uint64_t slots);
+void ckpt_init(CkptHeader &h);
+// exists=false and MCML_OK when the file is absent.
+int ckpt_read_header(const std::string &path, CkptHeader &h, bool &exists);
+int ckpt_read_records(const std::string &path, const CkptHeader &h, void *dst);
+// Writes h (with a fresh header digest) as the whole file's header.
+int ckpt_write_header(const std::string &path, CkptHeader &h);
+// Appends n records after the ones h counts, then the header that counts them.
+int ckpt_append(const std::string &path, CkptHeader &h, const void *recs, uint64_t n,
+                uint64_t slots_done, uint64_t steps);
 
 }  // namespace mcml

@@ -149,7 +149,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
 
   auto next_slot = [&]() -> bool {
     const uint64_t s = fetch_one(&A.counters[kCntSlot]);
-    if (s >= S) return false;
+    if (s >= A.slot_end) return false;
     slot = (uint32_t)s;
     load_state(st, A.slot_state, s);
     k = 0;

@@ -27,6 +27,7 @@ struct WalkArgs {
   unsigned long long *counters;  // kCntWords
   DetRecord *records;
   unsigned long long rec_cap;
+  unsigned long long slot_end;   // lanes stop taking slots here (<= num_slots)
 };
 
 struct ReplayArgs {

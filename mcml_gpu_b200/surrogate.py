@@ -175,7 +175,8 @@ def make_labels(base: Sim, *, n_baselines: int, photons: int, combos_per_baselin
     """White-MC labels: n_baselines tissues (mus drawn in mus_range, mua at
     the middle of its range) walked with `photons` photons and replayed;
     each replay relabelled to combos_per_baseline (mua', mus') with mua'
-    uniform in mua_range and mus' = mus * U(1 - mus_jitter, 1 + mus_jitter)."""
+    uniform in mua_range and mus' = mus * U(1 - mus_jitter, 1 + mus_jitter)
+    clipped to mus_range (so the training hull is the two ranges)."""
     rng = np.random.default_rng(seed)
     L, S = int(base.num_layers), int(base.num_sds)
     Xs, Ys, bl = [], [], []
@@ -191,8 +192,9 @@ def make_labels(base: Sim, *, n_baselines: int, photons: int, combos_per_baselin
             run.replay()
             rows = [run.rows(s) for s in range(1, S + 1)]
         combos = np.hstack([rng.uniform(*mua_range, (combos_per_baseline, L)),
-                            mus0[None, :] * rng.uniform(1 - mus_jitter, 1 + mus_jitter,
-                                                        (combos_per_baseline, L))]).astype(np.float32)
+                            np.clip(mus0[None, :] * rng.uniform(1 - mus_jitter, 1 + mus_jitter,
+                                                                (combos_per_baseline, L)),
+                                    *mus_range)]).astype(np.float32)
         R = np.stack([wmc.rescale(r, n, sim.mua[:L], sim.mus[:L], combos, photons,
                                   device=device).cpu().numpy() for r, n in rows], axis=1)
         feats = np.repeat(features([sim]), combos_per_baseline, axis=0)

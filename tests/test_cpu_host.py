@@ -151,3 +151,49 @@ def test_cli_bad_config_exits_1():
         r = run_cli(str(sj), str(it), "out.txt", cwd=td)
         assert r.returncode == 1
         assert "Something wrong with read_simulation_data!" in r.stdout
+
+
+def _fnv1a(data: bytes, h: int = 14695981039346656037) -> int:
+    for b in data:
+        h = ((h ^ b) * 1099511628211) & 0xFFFFFFFFFFFFFFFF
+    return h
+
+
+def _checkpoint_bytes(records: bytes, **f) -> bytes:
+    import struct
+    n = len(records) // 40
+    head = b"MCMLCKP1" + struct.pack("<II", 1, 40) + struct.pack(
+        "<10Q", f.get("digest", 7), f.get("seed", 5), 0, f.get("photons", 1000),
+        f.get("slots", 100), f.get("done", 40), n, f.get("steps", 123456), f.get("launches", 2),
+        _fnv1a(records))
+    return head + struct.pack("<Q", _fnv1a(head)) + bytes(24) + records
+
+
+def test_checkpoint_header_is_checked_on_the_host(tmp_path):
+    """The checkpoint layout documented in include/mcml_b200.h, written by
+    hand: read back field by field; a damaged header, a truncated record
+    area or another file is rejected with MCML_E_CHECKPOINT."""
+    import mcml_gpu_b200 as m
+    recs = bytes(range(200)) * 2  # ten 40-byte records
+    p = tmp_path / "a.ckpt"
+    p.write_bytes(_checkpoint_bytes(recs, seed=99, done=60, launches=3))
+    info = m.checkpoint_info(p)
+    assert (info.seed, info.photons, info.slots, info.slots_done, info.records, info.steps,
+            info.launches) == (99, 1000, 100, 60, 10, 123456, 3)
+    good = p.read_bytes()
+    bad = [good[:8] + bytes([2]) + good[9:],          # version
+           good[:30] + bytes([good[30] ^ 1]) + good[31:],  # header digest
+           good[:-1],                                  # truncated records
+           b"not a checkpoint" + good[16:]]
+    for b in bad:
+        p.write_bytes(b)
+        with pytest.raises(m.MCMLError) as e:
+            m.checkpoint_info(p)
+        assert e.value.status == -10
+    p.write_bytes(_checkpoint_bytes(recs, done=101))  # slots_done beyond slots
+    with pytest.raises(m.MCMLError) as e:
+        m.checkpoint_info(p)
+    assert e.value.status == -10
+    with pytest.raises(m.MCMLError) as e:
+        m.checkpoint_info(tmp_path / "missing.ckpt")
+    assert e.value.status == -5
