@@ -2,7 +2,7 @@
 """Throughput of the MCML photon-transport hot path on B200.
 
 One step = one pass of the hot path over the 5-layer benchmark tissue
-(tests/golden/configs/c1: heights 0.3/0.7/0.2/0.4/semi-infinite cm,
+(tests/golden/configs/five_layer: heights 0.3/0.7/0.2/0.4/semi-infinite cm,
 mua ~ U(0.05,0.5)/cm, mus ~ U(50,250)/cm drawn by seed, g=0.9, n=1.4,
 three oblique fibres at 0.8/1.5/3.0 cm): walk 1e8 photons, then replay
 every detected photon with per-layer pathlengths and the A_rz / A0_z
@@ -36,9 +36,9 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-CONFIG = ROOT / "tests" / "golden" / "configs" / "c1"
+CONFIG = ROOT / "tests" / "golden" / "configs" / "five_layer"
 METRIC = "photons/s (plain MC)"
-WORKLOAD = "plain MC + replay, 5-layer tissue, 1e8 photons, -R -A -B (config 1)"
+WORKLOAD = "plain MC + replay, 5-layer tissue, 1e8 photons, -R -A -B"
 
 # Per-step work of the walk, counted by hand from the step's arithmetic for
 # the common step (hop + weight drop + Henyey-Greenstein spin + roulette
@@ -228,8 +228,8 @@ def reference_gpu_arm(args) -> int:
 
 
 def batch_arm(args) -> int:
-    """Config 2: 4096 parameter sets of the 5-layer tissue (mua, mus drawn
-    from config 1's ranges by seed, photons log-uniform 1e5-1e7 per set) in
+    """Batched parameter sets: 4096 sets of the 5-layer tissue (mua, mus drawn
+    from the benchmark tissue's ranges by seed, photons log-uniform 1e5-1e7 per set) in
     one persistent CUDA-graph launch, autotuned; compared with the same sets
     run one after another (a sample of them, rate extrapolated)."""
     import torch
@@ -264,7 +264,7 @@ def batch_arm(args) -> int:
     print(json.dumps({
         "metric": "photons/s (batched plain MC)", "impl": "mcml-batch", "value": total / (ms / 1e3),
         "unit": "photons/s", "ms_per_step": ms, "steps": args.steps, "warmup": args.warmup,
-        "config": {"workload": "config 2: batched 5-layer sets, log-uniform photons per set",
+        "config": {"workload": "4096 batched 5-layer sets, log-uniform 1e5-1e7 photons per set",
                    "sets": n_sets, "photons_total": total,
                    "photons_per_set": [args.min_photons, args.max_photons],
                    "tuned": {"block": tuning.block_size, "blocks_per_sm": tuning.blocks_per_sm,
@@ -277,17 +277,18 @@ def batch_arm(args) -> int:
     return 0
 
 
-def reference_plain_mc_evals(cfg: Path, sims, photons: int) -> float | None:
+def reference_plain_mc_evals(cfg: Path, sims, photons: int) -> tuple[float | None, str]:
     """Plain-MC evaluations per second of the reference's CUDA build
-    (oracle/_ref/MCML_GPU) on the same tissues: one multi-simulation run,
-    wall clock from process start to exit."""
+    (oracle/_ref/MCML_GPU) on the same tissues, one process per tissue (its
+    multi-simulation mode ends in a segmentation fault here), wall clock
+    from process start to exit.  Returns (rate or None, note)."""
     import oracle
     if not oracle.REF_BIN.exists():
-        return None
+        return None, "oracle/_ref not built"
     conf = json.loads((cfg / "sim_set.json").read_text())
     conf["number_photons"] = photons
-    conf["number_simulation"] = len(sims)
-    lines = []
+    conf["number_simulation"] = 1
+    total = 0.0
     for s in sims:
         L = int(s.num_layers)
         vals = []
@@ -295,24 +296,26 @@ def reference_plain_mc_evals(cfg: Path, sims, photons: int) -> float | None:
             if l < L - 1:
                 vals.append(s.height[l])
             vals += [s.mua[l], s.mus[l], s.n[l], s.g[l]]
-        lines.append("\t".join(f"{float(v):.9g}" for v in vals))
-    with tempfile.TemporaryDirectory() as td:
-        (Path(td) / "sim_set.json").write_text(json.dumps(conf))
-        (Path(td) / "input.txt").write_text("\n".join(lines) + "\n")
-        env = dict(os.environ, MCML_FIXED_TIME="1234", LD_PRELOAD=str(oracle.REF_SHIM))
-        t0 = time.perf_counter()
-        res = subprocess.run([str(oracle.REF_BIN), "sim_set.json", "input.txt", "output.txt"],
-                             cwd=td, env=env, capture_output=True, text=True, timeout=3600)
-        dt = time.perf_counter() - t0
-    return len(sims) / dt if res.returncode == 0 else None
+        with tempfile.TemporaryDirectory() as td:
+            (Path(td) / "sim_set.json").write_text(json.dumps(conf))
+            (Path(td) / "input.txt").write_text("\t".join(f"{float(v):.9g}" for v in vals) + "\n")
+            env = dict(os.environ, MCML_FIXED_TIME="1234", LD_PRELOAD=str(oracle.REF_SHIM))
+            t0 = time.perf_counter()
+            res = subprocess.run([str(oracle.REF_BIN), "sim_set.json", "input.txt", "output.txt"],
+                                 cwd=td, env=env, capture_output=True, text=True, timeout=3600)
+            total += time.perf_counter() - t0
+        if res.returncode != 0:
+            tail = (res.stdout + res.stderr).strip().splitlines()[-3:]
+            return None, f"exit {res.returncode}: " + " | ".join(tail)
+    return len(sims) / total, f"{len(sims)} tissues x {photons:.3g} photons in {total:.2f} s"
 
 
-MUA_RANGE = (0.05, 0.5)   # 1/cm, config 1
-MUS_RANGE = (50.0, 250.0)  # 1/cm, config 1
+MUA_RANGE = (0.05, 0.5)   # 1/cm, the benchmark tissue's range
+MUS_RANGE = (50.0, 250.0)  # 1/cm
 
 
 def surrogate_arm(args) -> int:
-    """Configs 3-4: White-MC labels from replayed baselines of the 5-layer
+    """Surrogate training and serving: White-MC labels from replayed baselines of the 5-layer
     tissue (ring detectors at 0.5/1.0/1.5 cm, tests/golden/configs/surrogate),
     ensemble training on the GPU, serving of 1e6 queries (5 % outside the
     training hull, whose answers come from plain MC at 1e7 photons), and the
@@ -333,7 +336,7 @@ def surrogate_arm(args) -> int:
                              max_spread=0.05, fallback_photons=10_000_000)
     train_s = time.perf_counter() - t0
     rng = np.random.default_rng(5)
-    # 1e6 queries: mua and mus of every layer uniform over config 1's ranges;
+    # 1e6 queries: mua and mus of every layer uniform over the tissue's ranges;
     # 5 % of them take one coefficient from the 20 %-widened ranges' excess,
     # outside the training hull
     nq = args.queries
@@ -390,7 +393,7 @@ def surrogate_arm(args) -> int:
     logR, _ = sur.predict(sg.features(held))
     rel = np.abs(np.exp(logR) - R_ref) / R_ref
     mc_evals = mc_rate / float(args.ref_photons)
-    ref_evals = reference_plain_mc_evals(cfg, held[:2], int(args.ref_photons))
+    ref_evals, ref_note = reference_plain_mc_evals(cfg, held[:2], int(args.ref_photons))
     print(json.dumps({
         "metric": "SDS-reflectance evals/s", "impl": "mcml-surrogate",
         "value": nq / serve_s, "unit": "evals/s",
@@ -398,7 +401,7 @@ def surrogate_arm(args) -> int:
         "plain_mc_evals_per_s_at_ref_photons": mc_evals,
         "speedup_vs_plain_mc": (nq / serve_s) / mc_evals,
         "speedup_vs_plain_mc_inside_hull": (nq / mlp_s) / mc_evals,
-        "reference_plain_mc_evals_per_s": ref_evals,
+        "reference_plain_mc_evals_per_s": ref_evals, "reference_plain_mc_run": ref_note,
         "speedup_vs_reference_plain_mc": (nq / serve_s) / ref_evals if ref_evals else None,
         "fallback_fraction": float(fallback.mean()),
         "fallback_s_per_query_at_1e7": fb_per_query_s,
@@ -411,7 +414,7 @@ def surrogate_arm(args) -> int:
                    "photons_per_baseline": int(args.label_photons), "seconds": label_s},
         "training": {"epochs": args.epochs, "seconds": train_s,
                      "final_loss": [float(v) for v in sur.history[-1]]},
-        "config": {"workload": "configs 3-4: WMC labels, MLP 25->256x4->3 GELU, ensemble 4, "
+        "config": {"workload": "surrogate: WMC labels, MLP 25->256x4->3 GELU, ensemble 4, "
                                "BF16 tensor-core kernels; ring detectors 0.5/1.0/1.5 cm",
                    "queries": nq},
     }), flush=True)

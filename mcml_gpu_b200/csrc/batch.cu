@@ -1,7 +1,7 @@
 // batch.cu -- many tissue parameter sets in one persistent launch.
 //
 // The reference runs one simulation per launch sequence and its multi-set
-// mode is broken (SURVEY F7: critical_arr is only allocated for the first
+// mode is broken (critical_arr is only allocated for the first
 // simulation, io.cpp:193-197); a batch of parameter sets there means one
 // process per set.  Here all sets share one persistent walk launch:
 //

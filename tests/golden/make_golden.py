@@ -41,7 +41,7 @@ import oracle  # noqa: E402
 import mcml_gpu_b200 as mcml  # noqa: E402
 
 SEED = 20261203
-PARITY_CASES = ["fiber3", "ring5", "mismatch", "ringpt", "c0"]
+PARITY_CASES = ["fiber3", "ring5", "mismatch", "ringpt", "three_layer"]
 STREAM_PHOTONS_PER_SDS = 6
 
 

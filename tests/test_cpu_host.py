@@ -44,7 +44,7 @@ def test_version_and_strerror():
 
 
 def test_parse_reference_example():
-    sim = load_case("c0")
+    sim = load_case("three_layer")
     assert sim.num_layers == 3 and sim.num_sds == 3
     assert sim.number_photons == 1000000
     assert sim.source_probe_oblique == 1 and sim.detector_probe_oblique == 1
@@ -54,7 +54,7 @@ def test_parse_reference_example():
 
 
 def test_derived_constants():
-    sim = load_case("c0")
+    sim = load_case("three_layer")
     d = m.derive(sim)
     # Fresnel start weight at normal incidence, 1.457 -> 1.4 (io.cpp:230-237)
     r = ((1.457 - 1.4) / (1.457 + 1.4)) ** 2
@@ -76,8 +76,8 @@ def _write_case(td, sim_json, input_txt):
     return Path(td) / "s.json", Path(td) / "in.txt"
 
 
-BASE = json.loads((CONFIGS / "c0" / "sim_set.json").read_text())
-GOOD_INPUT = (CONFIGS / "c0" / "input.txt").read_text()
+BASE = json.loads((CONFIGS / "three_layer" / "sim_set.json").read_text())
+GOOD_INPUT = (CONFIGS / "three_layer" / "input.txt").read_text()
 
 
 @pytest.mark.parametrize("edit,text,message", [
@@ -111,14 +111,14 @@ def test_multi_simulation_file():
 def test_create_without_gpu_fails_cleanly():
     if m.device_count() > 0:
         pytest.skip("a GPU is present")
-    sim = load_case("c0")
+    sim = load_case("three_layer")
     with pytest.raises(m.MCMLError) as e:
         m.Simulation(sim)
     assert e.value.status == -9  # MCML_E_NODEV
 
 
 def test_invalid_sim_rejected_before_device_use():
-    sim = load_case("c0")
+    sim = load_case("three_layer")
     sim.num_layers = 11
     with pytest.raises(m.MCMLError) as e:
         m.Simulation(sim)
@@ -132,7 +132,7 @@ def run_cli(*args, cwd=None):
 def test_cli_usage_and_flag_rules():
     r = run_cli()
     assert r.returncode == 0 and "Usage:" in r.stderr
-    sj, it = CONFIGS / "c0" / "sim_set.json", CONFIGS / "c0" / "input.txt"
+    sj, it = CONFIGS / "three_layer" / "sim_set.json", CONFIGS / "three_layer" / "input.txt"
     for flags, msg in [(["-P"], "-P option only work with -R option!"),
                        (["-A"], "-A option only work with -R option!"),
                        (["-AP"], "-AP option only work with -R option!"),

@@ -7,7 +7,7 @@ count (one photon per thread, deterministic).  With the same seed and the
 same slot layout the library must reproduce:
   * the per-SDS detected counts exactly (SDS_detected_number);
   * every pathlength_SDS_#.bin row bit for bit (weight, per-layer
-    pathlength, steps) -- the north-star tolerance for pathlengths is
+    pathlength, steps) -- the required tolerance for pathlengths is
     1e-5 relative, the walk here meets 0;
   * A0_z_SDS_#.bin exactly and A_rz_SDS_#.bin by SHA-256;
   * average_pathlength.txt byte for byte (same rows, same FP64 formula);
@@ -29,7 +29,7 @@ from conftest import GOLDEN, load_case
 import mcml_gpu_b200 as m
 
 GOLDEN_DIR = Path(os.environ.get("MCML_GOLDEN_DIR", GOLDEN))
-CASES = ["fiber3", "ring5", "mismatch", "ringpt", "c0"]
+CASES = ["fiber3", "ring5", "mismatch", "ringpt", "three_layer"]
 
 
 def golden(case):

@@ -70,7 +70,7 @@ def test_oracle_first_pass_detects_reference_photons(case):
         assert s in [d[0] for d in dets], (s, k, dets)
 
 
-@pytest.mark.parametrize("case", CASES + ["c0"])
+@pytest.mark.parametrize("case", CASES + ["three_layer"])
 def test_reference_output_txt_is_float32_sum_of_rows(case):
     """Pins the reference's reflectance arithmetic: output.txt is the float32
     sum of the row weights in row order over 0xFFFFFFFF*N (io.cpp:11-33,
