@@ -423,6 +423,17 @@ int mcml_run_checkpointed(mcml_ctx *ctx, const mcml_checkpoint_opts *ck, mcml_re
 /* Reads and checks a checkpoint file on the host (no device needed). */
 int mcml_checkpoint_read_info(const char *path, mcml_checkpoint_info *info);
 
+/* ---- text formatting ---------------------------------------------------- */
+/*
+ * The text pathlength_SDS_#.txt holds for n_rows rows of row_len floats
+ * (io.cpp:313-323: every value in iostream's default format -- printf "%g",
+ * 6 significant digits -- followed by a tab, each row by a newline).  The
+ * text goes to out when it fits in capacity bytes; *written is its length
+ * either way (out may be NULL to size it).  Host only.
+ */
+int mcml_format_rows_text(const float *rows, uint64_t n_rows, uint32_t row_len, char *out,
+                          uint64_t capacity, uint64_t *written);
+
 /* ---- test support ------------------------------------------------------ */
 /*
  * The first count draws of curand_uniform on the XORWOW state

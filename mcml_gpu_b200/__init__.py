@@ -234,6 +234,8 @@ _SIGNATURES = [
     ("mcml_run_checkpointed", C.c_int, [C.c_void_p, C.POINTER(CheckpointOpts),
                                         C.POINTER(Result)]),
     ("mcml_checkpoint_read_info", C.c_int, [C.c_char_p, C.POINTER(CheckpointInfo)]),
+    ("mcml_format_rows_text", C.c_int, [C.c_void_p, C.c_uint64, C.c_uint32, C.c_void_p,
+                                        C.c_uint64, C.POINTER(C.c_uint64)]),
 ]
 
 
@@ -335,6 +337,20 @@ def shard(rank: int, world: int, photons: int, weak: bool = True) -> tuple[int, 
     base, extra = divmod(photons, world)
     n = base + (1 if rank < extra else 0)
     return rank * base + min(rank, extra), n
+
+
+def format_rows_text(rows: np.ndarray) -> bytes:
+    """The bytes of pathlength_SDS_#.txt for these rows (n x row_len float32)."""
+    lib = load_library()
+    rows = np.ascontiguousarray(rows, dtype=np.float32)
+    n, rl = (rows.shape[0], rows.shape[1]) if rows.ndim == 2 else (0, 1)
+    size = C.c_uint64()
+    _check(lib.mcml_format_rows_text(rows.ctypes.data, n, rl, None, 0, C.byref(size)),
+           "mcml_format_rows_text")
+    buf = C.create_string_buffer(max(int(size.value), 1))
+    _check(lib.mcml_format_rows_text(rows.ctypes.data, n, rl, buf, size.value, C.byref(size)),
+           "mcml_format_rows_text")
+    return buf.raw[:size.value]
 
 
 def checkpoint_info(path: os.PathLike | str) -> CheckpointInfo:

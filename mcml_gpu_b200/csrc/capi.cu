@@ -166,6 +166,7 @@ int set_sim(mcml_ctx *c, const mcml_sim *sim) {
   if (c->N / S >= 0xFFFFFFFFull)
     return set_error(MCML_E_INVALID, "too many photons per slot; raise mcml_opts.slots");
   if (S >= 0xFFFFFFFFull) return set_error(MCML_E_INVALID, "slots must be below 2^32");
+  if (c->N >= (1ull << 44)) return set_error(MCML_E_INVALID, "number_photons must be below 2^44");
   c->S = S;
   const uint64_t nz = grid_nz(c), nr = grid_nr(c);
   if (nr == 0 || nz == 0 || (uint64_t)sim->num_sds * nz * nr >= (1ull << 31))
@@ -239,6 +240,8 @@ int fill_result(mcml_ctx *c, mcml_result *r) {
   return MCML_OK;
 }
 
+// Records (and, after a replay, rows and interaction counts) to the host
+// in file order: by SDS, then photon index -- sorted on the device.
 int fetch_host(mcml_ctx *c) {
   if (c->host_valid) return MCML_OK;
   if (!c->ran) return set_error(MCML_E_STATE, "mcml_run has not been called");
@@ -248,33 +251,45 @@ int fetch_host(mcml_ctx *c) {
   CUDA_TRY(cudaStreamSynchronize(c->stream));
   if (cnt[kCntRecords] > c->rec_cap)
     return set_error(MCML_E_OVERFLOW, "detection records exceed capacity");
+  if (c->replayed && ((int)cnt[kCntStatus] & kStatusBudget))
+    return set_error(MCML_E_BUDGET, "a replayed photon exceeded the step budget");
   const uint64_t D = cnt[kCntRecords];
-  c->h_rec.resize(D);
-  if (D)
-    CUDA_TRY(cudaMemcpy(c->h_rec.data(), c->d_records, D * sizeof(DetRecord),
-                        cudaMemcpyDeviceToHost));
   const int L = (int)c->sim.num_layers;
-  if (c->replayed) {
-    if ((int)cnt[kCntStatus] & kStatusBudget)
-      return set_error(MCML_E_BUDGET, "a replayed photon exceeded the step budget");
-    c->h_rows.resize(D * (L + 2));
-    c->h_inter.resize(D * L);
-    if (D) {
-      CUDA_TRY(cudaMemcpy(c->h_rows.data(), c->d_rows, D * (L + 2) * sizeof(float),
-                          cudaMemcpyDeviceToHost));
-      CUDA_TRY(cudaMemcpy(c->h_inter.data(), c->d_inter, D * L * sizeof(uint32_t),
-                          cudaMemcpyDeviceToHost));
-    }
+  const bool rows = c->replayed;
+  c->h_rec.resize(D);
+  c->h_rows.resize(rows ? D * (L + 2) : 0);
+  c->h_inter.resize(rows ? D * L : 0);
+  if (D) {
+    DetRecord *rec = nullptr;
+    float *r = nullptr;
+    uint32_t *n = nullptr;
+    cudaError_t e = cudaMallocAsync(&rec, D * sizeof(DetRecord), c->stream);
+    if (e == cudaSuccess && rows) e = cudaMallocAsync(&r, D * (L + 2) * sizeof(float), c->stream);
+    if (e == cudaSuccess && rows) e = cudaMallocAsync(&n, D * L * sizeof(uint32_t), c->stream);
+    if (e == cudaSuccess)
+      e = sort_records_for_output(c->d_records, D, rows ? c->d_rows : nullptr, c->d_inter, L, rec,
+                                  r, n, c->sm_count, c->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(c->h_rec.data(), rec, D * sizeof(DetRecord), cudaMemcpyDeviceToHost,
+                          c->stream);
+    if (e == cudaSuccess && rows)
+      e = cudaMemcpyAsync(c->h_rows.data(), r, D * (L + 2) * sizeof(float),
+                          cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess && rows)
+      e = cudaMemcpyAsync(c->h_inter.data(), n, D * L * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                          c->stream);
+    if (n) cudaFreeAsync(n, c->stream);
+    if (r) cudaFreeAsync(r, c->stream);
+    if (rec) cudaFreeAsync(rec, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess)
+      return set_error(MCML_E_CUDA, std::string("ordering records: ") + cudaGetErrorString(e));
   }
   c->order.assign(c->sim.num_sds, {});
   for (uint64_t i = 0; i < D; ++i) {
     const uint32_t s = c->h_rec[i].sds;
     if (s >= 1 && s <= c->sim.num_sds) c->order[s - 1].push_back((uint32_t)i);
   }
-  for (auto &v : c->order)
-    std::sort(v.begin(), v.end(), [&](uint32_t a, uint32_t b) {
-      return c->h_rec[a].photon < c->h_rec[b].photon;
-    });
   c->host_valid = true;
   return MCML_OK;
 }

@@ -37,6 +37,13 @@ struct HostOutputs {
   float dr = 0.01f, dz = 0.01f;
 };
 
+// iostream's default text for a value (printf "%g": 6 significant digits,
+// C locale); at most kG6Max bytes.  put_row_text: the values of one
+// pathlength row, each followed by a tab, then a newline (io.cpp:313-323).
+constexpr int kG6Max = 16;
+char *put_g6(char *p, double v);
+char *put_row_text(char *p, const float *row, int row_len);
+
 // calculate_average_pathlength (transport.cu:274-297); out has S*L entries.
 void average_pathlength(const HostOutputs &o, std::vector<double> &out);
 

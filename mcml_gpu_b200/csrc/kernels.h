@@ -50,6 +50,14 @@ cudaError_t launch_walk(const DevParams &P, const WalkArgs &A, bool src_obl, boo
 const void *walk_kernel_ptr(int block, int min_blocks, bool src_obl, bool det_obl);
 cudaError_t launch_replay(const DevParams &P, const ReplayArgs &A, bool src_obl, bool det_obl,
                           bool ref_grid, int grid, cudaStream_t stream);
+// Copies the first D records -- and, when rows is not null, their replay
+// rows (L + 2 floats) and interaction counts (L words) -- into the *_out
+// buffers ordered by SDS, then photon index (order.cu).  Enqueued on
+// `stream`; scratch comes from the stream-ordered allocator.
+cudaError_t sort_records_for_output(const DetRecord *rec, uint64_t D, const float *rows,
+                                    const uint32_t *inter, int L, DetRecord *rec_out,
+                                    float *rows_out, uint32_t *inter_out, int sm_count,
+                                    cudaStream_t stream);
 cudaError_t launch_reduce_records(const DetRecord *rec, const unsigned long long *rec_count,
                                   unsigned long long rec_cap, unsigned n_sds,
                                   unsigned long long *det_count, double *wsum, double *wsq,

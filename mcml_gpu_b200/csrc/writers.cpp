@@ -6,10 +6,14 @@
 // caller-named reflectance file.  The value written for reflectance and
 // absorbance is computed with the reference's expressions
 // (weight / (0xFFFFFFFF*N), and / (scale*2*PI*(r+0.5)*dr*dr*dz)).
+#include <algorithm>
+#include <charconv>
 #include <cmath>
 #include <cstdio>
+#include <cstring>
 #include <fstream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "internal.h"
@@ -30,7 +34,51 @@ std::string numbered(const char *prefix, int sds1, const char *postfix) {
   return std::string(prefix) + std::to_string(sds1) + postfix;
 }
 
+// Text of lines [0, n) appended to fp.  line(i, p) writes line i at p (at
+// most max_line bytes) and returns its end.  Blocks of lines are formatted
+// by all host threads at once and written in order; per-line flushes of
+// the reference's `<< endl` only cost time, the bytes are the same.
+template <class Line>
+bool append_lines(FILE *fp, size_t n, size_t max_line, Line line) {
+  const size_t threads = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  const size_t block = std::max<size_t>(1, (size_t(4) << 20) / max_line);
+  std::vector<std::string> buf(threads);
+  std::vector<size_t> used(threads);
+  for (size_t base = 0; base < n; base += threads * block) {
+    auto work = [&](size_t t) {
+      const size_t i0 = base + t * block, i1 = std::min(n, i0 + block);
+      used[t] = 0;
+      if (i0 >= i1) return;
+      buf[t].resize((i1 - i0) * max_line);
+      char *p = &buf[t][0];
+      for (size_t i = i0; i < i1; ++i) p = line(i, p);
+      used[t] = (size_t)(p - &buf[t][0]);
+    };
+    const size_t active = std::min(threads, (n - base + block - 1) / block);
+    std::vector<std::thread> pool;
+    for (size_t t = 1; t < active; ++t) pool.emplace_back(work, t);
+    work(0);
+    for (auto &th : pool) th.join();
+    for (size_t t = 0; t < active; ++t)
+      if (used[t] && std::fwrite(buf[t].data(), 1, used[t], fp) != used[t]) return false;
+  }
+  return true;
+}
+
 }  // namespace
+
+char *put_g6(char *p, double v) {
+  return std::to_chars(p, p + kG6Max, v, std::chars_format::general, 6).ptr;
+}
+
+char *put_row_text(char *p, const float *row, int row_len) {
+  for (int j = 0; j < row_len; ++j) {
+    p = put_g6(p, row[j]);
+    *p++ = '\t';
+  }
+  *p++ = '\n';
+  return p;
+}
 
 // transport.cu:274-297
 void average_pathlength(const HostOutputs &o, std::vector<double> &out) {
@@ -116,14 +164,15 @@ int write_pathlength(const HostOutputs &o, const std::string &dir, bool binary) 
       if (!ok) return set_error(MCML_E_IO, "write failed: " + name);
     } else {
       const std::string name = join(dir, numbered("pathlength_SDS_", s + 1, ".txt"));
-      std::ofstream f(name, std::ios::app);
-      if (!f) return set_error(MCML_E_IO, "cannot open " + name);
-      const size_t n = rows.size() / (size_t)(L + 2);
-      for (size_t i = 0; i < n; i++) {
-        for (int j = 0; j <= L + 1; j++) f << rows[i * (L + 2) + j] << '\t';
-        f << std::endl;
-      }
-      if (!f) return set_error(MCML_E_IO, "write failed: " + name);
+      FILE *fp = std::fopen(name.c_str(), "ab");
+      if (!fp) return set_error(MCML_E_IO, "cannot open " + name);
+      const int rl = L + 2;
+      const size_t n = rows.size() / (size_t)rl;
+      const bool ok = append_lines(fp, n, (size_t)rl * (kG6Max + 1) + 1, [&](size_t i, char *p) {
+        return put_row_text(p, &rows[i * rl], rl);
+      });
+      const bool closed = std::fclose(fp) == 0;
+      if (!ok || !closed) return set_error(MCML_E_IO, "write failed: " + name);
     }
   }
   return MCML_OK;
@@ -164,13 +213,18 @@ int write_A_rz(const HostOutputs &o, const std::string &dir, bool binary) {
       if (!ok) return set_error(MCML_E_IO, "write failed: " + name);
     } else {
       const std::string name = join(dir, numbered("A_rz_SDS_", s + 1, ".txt"));
-      std::ofstream f(name, std::ios::app);
-      if (!f) return set_error(MCML_E_IO, "cannot open " + name);
-      for (uint32_t z = 0; z < nz; z++) {
-        for (uint32_t r = 0; r < nr; r++) f << double(data[(size_t)z * nr + r] / scale2[r]) << "\t";
-        f << std::endl;
-      }
-      if (!f) return set_error(MCML_E_IO, "write failed: " + name);
+      FILE *fp = std::fopen(name.c_str(), "ab");
+      if (!fp) return set_error(MCML_E_IO, "cannot open " + name);
+      const bool ok = append_lines(fp, nz, (size_t)nr * (kG6Max + 1) + 1, [&](size_t z, char *p) {
+        for (uint32_t r = 0; r < nr; r++) {
+          p = put_g6(p, double(data[z * nr + r] / scale2[r]));
+          *p++ = '\t';
+        }
+        *p++ = '\n';
+        return p;
+      });
+      const bool closed = std::fclose(fp) == 0;
+      if (!ok || !closed) return set_error(MCML_E_IO, "write failed: " + name);
     }
   }
   return MCML_OK;
@@ -194,13 +248,38 @@ int write_A0_z(const HostOutputs &o, const std::string &dir, bool binary) {
       if (!ok) return set_error(MCML_E_IO, "write failed: " + name);
     } else {
       const std::string name = join(dir, numbered("A0_z_SDS_", s + 1, ".txt"));
-      std::ofstream f(name, std::ios::app);
-      if (!f) return set_error(MCML_E_IO, "cannot open " + name);
-      for (uint32_t z = 0; z < nz; z++) f << double(data[z] / scale2) << std::endl;
-      if (!f) return set_error(MCML_E_IO, "write failed: " + name);
+      FILE *fp = std::fopen(name.c_str(), "ab");
+      if (!fp) return set_error(MCML_E_IO, "cannot open " + name);
+      const bool ok = append_lines(fp, nz, kG6Max + 2, [&](size_t z, char *p) {
+        p = put_g6(p, double(data[z] / scale2));
+        *p++ = '\n';
+        return p;
+      });
+      const bool closed = std::fclose(fp) == 0;
+      if (!ok || !closed) return set_error(MCML_E_IO, "write failed: " + name);
     }
   }
   return MCML_OK;
 }
 
 }  // namespace mcml
+
+using namespace mcml;
+
+extern "C" int mcml_format_rows_text(const float *rows, uint64_t n_rows, uint32_t row_len,
+                                     char *out, uint64_t capacity, uint64_t *written) {
+  clear_error();
+  if ((!rows && n_rows) || !written || row_len == 0)
+    return set_error(MCML_E_INVALID, "bad argument");
+  char line[64 * (kG6Max + 1)];
+  if (row_len > 63) return set_error(MCML_E_INVALID, "row_len above 63");
+  uint64_t total = 0;
+  for (uint64_t i = 0; i < n_rows; ++i) {
+    const size_t len = (size_t)(put_row_text(line, rows + i * row_len, (int)row_len) - line);
+    if (out && total + len <= capacity) std::memcpy(out + total, line, len);
+    total += len;
+  }
+  *written = total;
+  return (!out || total <= capacity) ? MCML_OK
+                                     : set_error(MCML_E_INVALID, "output buffer too small");
+}

@@ -197,3 +197,22 @@ def test_checkpoint_header_is_checked_on_the_host(tmp_path):
     with pytest.raises(m.MCMLError) as e:
         m.checkpoint_info(tmp_path / "missing.ckpt")
     assert e.value.status == -5
+
+
+def test_row_text_matches_iostream_default_format():
+    """pathlength_SDS_#.txt text: every float as iostream prints it by
+    default (printf "%g", 6 significant digits), tab after each value,
+    newline after each row -- checked against Python's %g over random bit
+    patterns of every float class and the values rows really hold."""
+    import mcml_gpu_b200 as m
+    rng = np.random.default_rng(3)
+    bits = rng.integers(0, 2**32, size=(20000, 7), dtype=np.uint64).astype(np.uint32)
+    rows = bits.view(np.float32).copy()
+    rows[np.isnan(rows)] = 1.5
+    special = np.array([[0.0, -0.0, np.inf, -np.inf, 4294967295.0, 1e-45, 3.4028235e38],
+                        [123456.5, 999999.5, 9999995.0, 0.0001, 1e-5, 100000.0, 1e6]],
+                       np.float32)
+    rows = np.vstack([rows, special])
+    want = "".join("".join("%g\t" % float(v) for v in r) + "\n" for r in rows).encode()
+    assert m.format_rows_text(rows) == want
+    assert m.format_rows_text(np.zeros((0, 7), np.float32)) == b""

@@ -2,7 +2,7 @@
 on the GPU -> served predictions, compared with plain MC.
 
 The held-out tissues are drawn like the labels (a baseline's scattering
-within a few percent, absorption anywhere in range).  The network must
+within a few percent, clipped to 50-250 /cm, absorption anywhere in range).  The network must
 (a) agree with plain MC walked at 2e7 photons per tissue within 6 %
 median relative error (measured: 1.6 %, with the reference's own
 standard error at 0.4 %), and (b) beat plain MC given the same GPU time as
@@ -34,7 +34,7 @@ def held_out(labels, count, rng, mua_range=(0.05, 0.5), jitter=0.05):
         s = m.Sim.from_buffer_copy(b)
         for l in range(L):
             s.mua[l] = float(rng.uniform(*mua_range))
-            s.mus[l] = float(b.mus[l] * rng.uniform(1 - jitter, 1 + jitter))
+            s.mus[l] = float(np.clip(b.mus[l] * rng.uniform(1 - jitter, 1 + jitter), 50.0, 250.0))
         out.append(s)
     return out
 
