@@ -423,6 +423,29 @@ int mcml_run_checkpointed(mcml_ctx *ctx, const mcml_checkpoint_opts *ck, mcml_re
 /* Reads and checks a checkpoint file on the host (no device needed). */
 int mcml_checkpoint_read_info(const char *path, mcml_checkpoint_info *info);
 
+/* ---- outputs from host data ------------------------------------------- */
+/*
+ * The same files as mcml_write_outputs, from host arrays instead of a
+ * context: for results combined from several runs (replicas over
+ * disjoint slot ranges on several GPUs, concatenated in slot order) or
+ * kept from an earlier run.  Host only; no device is touched.
+ */
+typedef struct mcml_host_data {
+  uint64_t photons;          /* the combined run's photon count (output scales)      */
+  const uint64_t *detected;  /* num_sds detected counts                              */
+  const double *weight_sum;  /* num_sds FP64 sums of detected weights (quanta)       */
+  const float *const *rows;  /* num_sds pointers to detected[s] rows of L+2 floats,
+                                photon order (pathlength_SDS_#); NULL without -R     */
+  const uint64_t *A_rz;      /* num_sds x nz x nr u64 quanta, or NULL                */
+  const uint64_t *A0_z;      /* num_sds x nz u64 quanta, or NULL                     */
+  uint32_t grid_nr, grid_nz; /* 0 = the reference grid                               */
+  float grid_dr, grid_dz;
+  const char *gpu_name;      /* summary.json "sim_GPU"                               */
+} mcml_host_data;
+int mcml_write_host_outputs(const mcml_sim *sim, const mcml_host_data *data, const char *dir,
+                            const char *output_txt, uint32_t flags, double sim_s,
+                            double replay_s);
+
 /* ---- text formatting ---------------------------------------------------- */
 /*
  * The text pathlength_SDS_#.txt holds for n_rows rows of row_len floats

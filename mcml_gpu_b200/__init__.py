@@ -190,6 +190,22 @@ class CheckpointInfo(C.Structure):
                                           "records", "steps", "launches")]
 
 
+class HostData(C.Structure):
+    _fields_ = [
+        ("photons", C.c_uint64),
+        ("detected", C.c_void_p),
+        ("weight_sum", C.c_void_p),
+        ("rows", C.c_void_p),
+        ("A_rz", C.c_void_p),
+        ("A0_z", C.c_void_p),
+        ("grid_nr", C.c_uint32),
+        ("grid_nz", C.c_uint32),
+        ("grid_dr", C.c_float),
+        ("grid_dz", C.c_float),
+        ("gpu_name", C.c_char_p),
+    ]
+
+
 INCOMPLETE = 1  # MCML_INCOMPLETE: a checkpointed run stopped early
 
 _lib: Optional[C.CDLL] = None
@@ -234,6 +250,8 @@ _SIGNATURES = [
     ("mcml_run_checkpointed", C.c_int, [C.c_void_p, C.POINTER(CheckpointOpts),
                                         C.POINTER(Result)]),
     ("mcml_checkpoint_read_info", C.c_int, [C.c_char_p, C.POINTER(CheckpointInfo)]),
+    ("mcml_write_host_outputs", C.c_int, [C.POINTER(Sim), C.POINTER(HostData), C.c_char_p,
+                                          C.c_char_p, C.c_uint32, C.c_double, C.c_double]),
     ("mcml_format_rows_text", C.c_int, [C.c_void_p, C.c_uint64, C.c_uint32, C.c_void_p,
                                         C.c_uint64, C.POINTER(C.c_uint64)]),
 ]

@@ -837,28 +837,7 @@ int mcml_write_outputs(mcml_ctx *ctx, const char *dir, const char *output_txt, u
   }
   build_outputs(ctx, o, arz, a0z);
   o.replayed = replay;
-  const std::string d = dir ? dir : "";
-  const bool bin = (flags & MCML_OUT_BINARY) != 0;
-  auto path = [&](const char *name) { return d.empty() ? std::string(name) : d + "/" + name; };
-  if (replay) {
-    if (flags & MCML_OUT_PATHLENGTH) {
-      rc = write_pathlength(o, d, bin);
-      if (rc) return rc;
-    }
-    if (flags & MCML_OUT_AVERAGE_PL) {
-      rc = write_average_pathlength(o, path("average_pathlength.txt"));
-      if (rc) return rc;
-    }
-  }
-  rc = write_output_txt(o, output_txt);
-  if (rc) return rc;
-  if (replay && (flags & MCML_OUT_ABSORBANCE)) {
-    rc = write_A_rz(o, d, bin);
-    if (rc) return rc;
-    rc = write_A0_z(o, d, bin);
-    if (rc) return rc;
-  }
-  return write_summary(o, path("summary.json"), sim_s, replay_s);
+  return write_files(o, dir ? dir : "", output_txt, flags, sim_s, replay_s);
 }
 
 int mcml_uniform_stream(int device, uint64_t seed, uint64_t subsequence, uint64_t count,

@@ -55,6 +55,12 @@ int write_average_pathlength(const HostOutputs &o, const std::string &path);
 int write_A_rz(const HostOutputs &o, const std::string &dir, bool binary);
 int write_A0_z(const HostOutputs &o, const std::string &dir, bool binary);
 
+// The files of one simulation as mcml_write_outputs writes them (flags:
+// MCML_OUT_*; pathlength, average pathlength and absorbance only with
+// MCML_OUT_REPLAY, io.cpp:281-469 and main.cu:108-141).
+int write_files(const HostOutputs &o, const std::string &dir, const char *output_txt,
+                uint32_t flags, double sim_s, double replay_s);
+
 // Checkpoint file of a chunked first pass (checkpoint.cpp); the layout is
 // the one documented beside mcml_run_checkpointed.
 constexpr uint64_t kFnvBasis = 14695981039346656037ull;

@@ -262,6 +262,32 @@ int write_A0_z(const HostOutputs &o, const std::string &dir, bool binary) {
   return MCML_OK;
 }
 
+int write_files(const HostOutputs &o, const std::string &d, const char *output_txt,
+                uint32_t flags, double sim_s, double replay_s) {
+  const bool replay = (flags & MCML_OUT_REPLAY) != 0;
+  const bool bin = (flags & MCML_OUT_BINARY) != 0;
+  int rc;
+  if (replay) {
+    if (flags & MCML_OUT_PATHLENGTH) {
+      rc = write_pathlength(o, d, bin);
+      if (rc) return rc;
+    }
+    if (flags & MCML_OUT_AVERAGE_PL) {
+      rc = write_average_pathlength(o, join(d, "average_pathlength.txt"));
+      if (rc) return rc;
+    }
+  }
+  rc = write_output_txt(o, output_txt);
+  if (rc) return rc;
+  if (replay && (flags & MCML_OUT_ABSORBANCE)) {
+    rc = write_A_rz(o, d, bin);
+    if (rc) return rc;
+    rc = write_A0_z(o, d, bin);
+    if (rc) return rc;
+  }
+  return write_summary(o, join(d, "summary.json"), sim_s, replay_s);
+}
+
 }  // namespace mcml
 
 using namespace mcml;
@@ -282,4 +308,45 @@ extern "C" int mcml_format_rows_text(const float *rows, uint64_t n_rows, uint32_
   *written = total;
   return (!out || total <= capacity) ? MCML_OK
                                      : set_error(MCML_E_INVALID, "output buffer too small");
+}
+
+extern "C" int mcml_write_host_outputs(const mcml_sim *sim, const mcml_host_data *d,
+                                       const char *dir, const char *output_txt, uint32_t flags,
+                                       double sim_s, double replay_s) {
+  clear_error();
+  if (!sim || !d || !output_txt || !d->detected || !d->weight_sum)
+    return set_error(MCML_E_INVALID, "null argument");
+  const bool replay = (flags & MCML_OUT_REPLAY) != 0;
+  if (replay && !d->rows) return set_error(MCML_E_INVALID, "replay outputs need rows");
+  if (replay && (flags & MCML_OUT_ABSORBANCE) && (!d->A_rz || !d->A0_z))
+    return set_error(MCML_E_INVALID, "absorbance outputs need A_rz and A0_z");
+  int rc = validate_sim(sim);
+  if (rc) return rc;
+  mcml_sim s = *sim;
+  s.number_photons = d->photons;
+  mcml_derived der;
+  rc = derive(&s, &der);
+  if (rc) return rc;
+  HostOutputs o;
+  o.sim = &s;
+  o.der = &der;
+  o.gpu_name = d->gpu_name ? d->gpu_name : "";
+  o.replayed = replay;
+  const unsigned S = s.num_sds;
+  const int L = (int)s.num_layers;
+  o.weight_sum.assign(d->weight_sum, d->weight_sum + S);
+  o.detected.assign(d->detected, d->detected + S);
+  o.rows.assign(S, {});
+  if (replay)
+    for (unsigned k = 0; k < S; ++k) {
+      if (d->detected[k] && !d->rows[k]) return set_error(MCML_E_INVALID, "missing rows");
+      o.rows[k].assign(d->rows[k], d->rows[k] + d->detected[k] * (uint64_t)(L + 2));
+    }
+  o.nr = d->grid_nr ? d->grid_nr : MCML_REF_GRID_NR;
+  o.nz = d->grid_nz ? d->grid_nz : MCML_REF_GRID_NZ;
+  o.dr = d->grid_dr > 0 ? d->grid_dr : MCML_REF_GRID_D;
+  o.dz = d->grid_dz > 0 ? d->grid_dz : MCML_REF_GRID_D;
+  o.A_rz = d->A_rz;
+  o.A0_z = d->A0_z;
+  return write_files(o, dir ? dir : "", output_txt, flags, sim_s, replay_s);
 }
