@@ -200,7 +200,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) batch_walk_kernel(const Ba
     }
     if (s > 0.0f) {
       const float4 L = t.lay[p.layer];
-      drop_weight(p, L.w, L.z);
+      drop_weight_walk(p, L.w, L.z);
       spin(p, t.lay2[p.layer].x, &st);
     }
     if (!survive<true>(p, &st)) {

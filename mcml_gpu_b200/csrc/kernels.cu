@@ -166,10 +166,13 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
   launch_photon<kSrcOblique>(p, &st, t, start_w);
 
   for (;;) {
+    // The photon's layer record, read once per step: hop, clamp and (when
+    // no boundary was hit, so the layer is unchanged) drop all use it.
+    const float4 L = t.lay[p.layer];
     float s;
-    const int new_layer = hop(p, s, &st, t);
+    const int new_layer = hop(p, s, &st, L);
     p.steps++;
-    clamp_z(p, t, p.layer);
+    clamp_z(p, L);
 
     if (new_layer != p.layer) {
       const int temp_layer = p.layer;
@@ -211,8 +214,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
     }
 
     if (s > 0.0f) {
-      const float4 L = t.lay[p.layer];
-      drop_weight(p, L.w, L.z);
+      drop_weight_walk(p, L.w, L.z);
       spin(p, t.lay2[p.layer].x, &st);
     }
 
