@@ -43,23 +43,26 @@ WORKLOAD = "plain MC + replay, 5-layer tissue, 1e8 photons, -R -A -B"
 # Per-step work of the walk, counted by hand from the step's arithmetic for
 # the common step (hop + weight drop + Henyey-Greenstein spin + roulette
 # test; no boundary, no roulette draw):
-#   3 XORWOW draws: 9 integer ops + 1 FMA each (lane), 1 int->float (XU)
-#   hop: 2 mul, 2 fma + 2 cmp (boundary), 3 fma (move), 1 add, 4 clamp,
-#        1 cmp (lane); lg2 (XU)
-#   drop: 2 mul, 1 sub (lane); 2 float->int, 2 int->float (XU)
-#   spin: HG 10, two IEEE sqrt 2x5, sincos 2, rotation 15, renormalise 6,
-#        1 cmp (lane); 2 rcp, 2 rsq (sqrt), sin, cos, 2 rcp, rsq (XU)
-#   survive: 2 cmp (lane)
-# = 94 FP32/INT32 lane ops and 17 quarter-rate (MUFU + conversion) ops.
-# A B200 SM issues 128 thread-instructions and 16 XU results per clock, so
-# steps/s <= f_sm * 148 * min(128 / (94 + 17), 16 / 17): the XU pipe binds.
-OPS_LANE = 94
-OPS_XU = 17
+#   3 XORWOW draws: 9 integer ops, 1 int->float, 1 FMA each      33 lane
+#   hop: 2 mul, 2 fma + 2 cmp (boundary), 3 fma (move), steps++,
+#        4 clamp, 1 layer cmp                                    15 lane, lg2
+#   drop: 2 mul, rint, sub                                        4 lane
+#   spin: HG 10, two IEEE sqrt 2x5, sincos 2, rotation 15,
+#        renormalise 6, 1 cmp                                    44 lane;
+#        rcp x3, rsq x2 (sqrt), sin, cos, rsq                     8 MUFU
+#   survive: 2 cmp                                                2 lane
+# = 98 FP32/INT32 lane ops and 9 MUFU ops.  A B200 SM issues 128
+# thread-instructions per clock (4 schedulers x 32 lanes) and 16 MUFU
+# results, so steps/s <= f_sm * 148 * min(128 / (98 + 9), 16 / 9): the
+# issue rate binds.  ncu's pipe counters agree that MUFU is not the limit:
+# 9.6 XU thread-instructions per step, 90 % of issue slots used.
+OPS_LANE = 98
+OPS_MUFU = 9
 SM_COUNT = 148
 
 
 def steps_per_clock_per_sm() -> float:
-    return min(128.0 / (OPS_LANE + OPS_XU), 16.0 / OPS_XU)
+    return min(128.0 / (OPS_LANE + OPS_MUFU), 16.0 / OPS_MUFU)
 
 
 class ClockSampler:
@@ -554,8 +557,9 @@ def mcml_arm(args) -> int:
                      "traffic": read_traffic(int(res.slots)),
                      "kernel": "walk_kernel",
                      "model": f"steps/s <= f_sm x {info.sm_count} SMs x min(128/({OPS_LANE}+"
-                              f"{OPS_XU}), 16/{OPS_XU}) at the measured median SM clock "
-                              f"(XU-pipe bound); ops counted by hand per common step",
+                              f"{OPS_MUFU}), 16/{OPS_MUFU}) at the measured median SM clock "
+                              f"(issue bound: 128 thread-instructions/clk/SM); ops counted "
+                              f"by hand per common step",
                      "walk_ms": walk_kernel_ms, "seed_ms": float(res.seed_ms),
                      "replay_ms": float(rep.replay_ms)},
         "clocks": clocks,

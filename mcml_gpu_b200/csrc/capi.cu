@@ -97,6 +97,8 @@ struct mcml_ctx {
   unsigned long long *d_Arz = nullptr;
   unsigned long long *d_A0z = nullptr;
   size_t arz_n = 0, a0z_n = 0;
+  void *d_order = nullptr;  // record-ordering scratch (fetch_host)
+  size_t order_bytes = 0;
   // [0] first pass start, [4] walk start, [1] walk end, [2]/[3] replay
   cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   int walk_block = 128;
@@ -121,6 +123,7 @@ struct mcml_ctx {
     dfree(d_inter);
     dfree(d_Arz);
     dfree(d_A0z);
+    dfree(d_order);
     for (auto &e : ev)
       if (e) cudaEventDestroy(e);
     if (own_stream && stream) cudaStreamDestroy(stream);
@@ -260,30 +263,26 @@ int fetch_host(mcml_ctx *c) {
   c->h_rows.resize(rows ? D * (L + 2) : 0);
   c->h_inter.resize(rows ? D * L : 0);
   if (D) {
-    DetRecord *rec = nullptr;
-    float *r = nullptr;
-    uint32_t *n = nullptr;
-    cudaError_t e = cudaMallocAsync(&rec, D * sizeof(DetRecord), c->stream);
-    if (e == cudaSuccess && rows) e = cudaMallocAsync(&r, D * (L + 2) * sizeof(float), c->stream);
-    if (e == cudaSuccess && rows) e = cudaMallocAsync(&n, D * L * sizeof(uint32_t), c->stream);
-    if (e == cudaSuccess)
-      e = sort_records_for_output(c->d_records, D, rows ? c->d_rows : nullptr, c->d_inter, L, rec,
-                                  r, n, c->sm_count, c->stream);
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(c->h_rec.data(), rec, D * sizeof(DetRecord), cudaMemcpyDeviceToHost,
-                          c->stream);
-    if (e == cudaSuccess && rows)
-      e = cudaMemcpyAsync(c->h_rows.data(), r, D * (L + 2) * sizeof(float),
-                          cudaMemcpyDeviceToHost, c->stream);
-    if (e == cudaSuccess && rows)
-      e = cudaMemcpyAsync(c->h_inter.data(), n, D * L * sizeof(uint32_t), cudaMemcpyDeviceToHost,
-                          c->stream);
-    if (n) cudaFreeAsync(n, c->stream);
-    if (r) cudaFreeAsync(r, c->stream);
-    if (rec) cudaFreeAsync(rec, c->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-    if (e != cudaSuccess)
-      return set_error(MCML_E_CUDA, std::string("ordering records: ") + cudaGetErrorString(e));
+    // Ordering scratch: kept by the context and grown, never shrunk.
+    const size_t need = order_scratch_bytes(D, L, rows);
+    if (need > c->order_bytes) {
+      dfree(c->d_order);
+      c->order_bytes = 0;
+      CUDA_TRY(cudaMalloc(&c->d_order, need));
+      c->order_bytes = need;
+    }
+    OrderedOutput o;
+    CUDA_TRY(sort_records_for_output(c->d_records, D, rows ? c->d_rows : nullptr, c->d_inter, L,
+                                     c->d_order, c->order_bytes, &o, c->sm_count, c->stream));
+    CUDA_TRY(cudaMemcpyAsync(c->h_rec.data(), o.records, D * sizeof(DetRecord),
+                             cudaMemcpyDeviceToHost, c->stream));
+    if (rows) {
+      CUDA_TRY(cudaMemcpyAsync(c->h_rows.data(), o.rows, D * (L + 2) * sizeof(float),
+                               cudaMemcpyDeviceToHost, c->stream));
+      CUDA_TRY(cudaMemcpyAsync(c->h_inter.data(), o.interactions, D * L * sizeof(uint32_t),
+                               cudaMemcpyDeviceToHost, c->stream));
+    }
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
   }
   c->order.assign(c->sim.num_sds, {});
   for (uint64_t i = 0; i < D; ++i) {

@@ -50,13 +50,20 @@ cudaError_t launch_walk(const DevParams &P, const WalkArgs &A, bool src_obl, boo
 const void *walk_kernel_ptr(int block, int min_blocks, bool src_obl, bool det_obl);
 cudaError_t launch_replay(const DevParams &P, const ReplayArgs &A, bool src_obl, bool det_obl,
                           bool ref_grid, int grid, cudaStream_t stream);
-// Copies the first D records -- and, when rows is not null, their replay
-// rows (L + 2 floats) and interaction counts (L words) -- into the *_out
-// buffers ordered by SDS, then photon index (order.cu).  Enqueued on
-// `stream`; scratch comes from the stream-ordered allocator.
+// The first D records -- and, when rows is not null, their replay rows
+// (L + 2 floats) and interaction counts (L words) -- ordered by SDS, then
+// photon index, in caller-provided device scratch of at least
+// order_scratch_bytes(D, L, rows != nullptr) bytes (order.cu).  The
+// ordered arrays are placed in the scratch; *out points at them.
+struct OrderedOutput {
+  DetRecord *records = nullptr;
+  float *rows = nullptr;
+  uint32_t *interactions = nullptr;
+};
+size_t order_scratch_bytes(uint64_t D, int L, bool rows);
 cudaError_t sort_records_for_output(const DetRecord *rec, uint64_t D, const float *rows,
-                                    const uint32_t *inter, int L, DetRecord *rec_out,
-                                    float *rows_out, uint32_t *inter_out, int sm_count,
+                                    const uint32_t *inter, int L, void *scratch,
+                                    size_t scratch_bytes, OrderedOutput *out, int sm_count,
                                     cudaStream_t stream);
 cudaError_t launch_reduce_records(const DetRecord *rec, const unsigned long long *rec_count,
                                   unsigned long long rec_cap, unsigned n_sds,

@@ -43,39 +43,60 @@ __global__ void gather_kernel(const uint32_t *perm, uint64_t D, const DetRecord 
   }
 }
 
+size_t align256(size_t n) { return (n + 255) & ~size_t(255); }
+
+size_t cub_temp_bytes(uint64_t D) {
+  size_t bytes = 0;
+  uint64_t *k = nullptr;
+  uint32_t *v = nullptr;
+  cub::DeviceRadixSort::SortPairs(nullptr, bytes, k, k, v, v, (int)D, 0, kPhotonBits + 5);
+  return bytes;
+}
+
 }  // namespace
 
+size_t order_scratch_bytes(uint64_t D, int L, bool rows) {
+  if (D == 0) return 0;
+  size_t b = align256(2 * D * sizeof(uint64_t)) + align256(2 * D * sizeof(uint32_t)) +
+             align256(cub_temp_bytes(D)) + align256(D * sizeof(DetRecord));
+  if (rows) b += align256(D * (L + 2) * sizeof(float)) + align256(D * L * sizeof(uint32_t));
+  return b;
+}
+
 cudaError_t sort_records_for_output(const DetRecord *rec, uint64_t D, const float *rows,
-                                    const uint32_t *inter, int L, DetRecord *rec_out,
-                                    float *rows_out, uint32_t *inter_out, int sm_count,
+                                    const uint32_t *inter, int L, void *scratch,
+                                    size_t scratch_bytes, OrderedOutput *out, int sm_count,
                                     cudaStream_t stream) {
+  *out = OrderedOutput{};
   if (D == 0) return cudaSuccess;
   if (D >= (1ull << 31)) return cudaErrorInvalidValue;
-  uint64_t *keys = nullptr;
-  uint32_t *idx = nullptr;
-  void *temp = nullptr;
-  size_t temp_bytes = 0;
-  cudaError_t e = cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, keys, keys, idx, idx,
-                                                  (int)D, 0, kPhotonBits + 5, stream);
-  if (e == cudaSuccess) e = cudaMallocAsync(&keys, 2 * D * sizeof(uint64_t), stream);
-  if (e == cudaSuccess) e = cudaMallocAsync(&idx, 2 * D * sizeof(uint32_t), stream);
-  if (e == cudaSuccess) e = cudaMallocAsync(&temp, temp_bytes, stream);
-  if (e == cudaSuccess) {
-    const int grid = 4 * sm_count;
-    record_keys_kernel<<<grid, 256, 0, stream>>>(rec, D, keys, idx);
-    e = cudaGetLastError();
-    if (e == cudaSuccess)
-      e = cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys, keys + D, idx, idx + D, (int)D,
-                                          0, kPhotonBits + 5, stream);
-    if (e == cudaSuccess) {
-      gather_kernel<<<grid, 256, 0, stream>>>(idx + D, D, rec, rec_out, rows, rows_out, inter,
-                                              inter_out, L);
-      e = cudaGetLastError();
-    }
+  if (scratch_bytes < order_scratch_bytes(D, L, rows != nullptr)) return cudaErrorInvalidValue;
+  char *p = static_cast<char *>(scratch);
+  auto take = [&](size_t n) {
+    char *q = p;
+    p += align256(n);
+    return q;
+  };
+  uint64_t *keys = reinterpret_cast<uint64_t *>(take(2 * D * sizeof(uint64_t)));
+  uint32_t *idx = reinterpret_cast<uint32_t *>(take(2 * D * sizeof(uint32_t)));
+  size_t temp_bytes = cub_temp_bytes(D);
+  void *temp = take(temp_bytes);
+  out->records = reinterpret_cast<DetRecord *>(take(D * sizeof(DetRecord)));
+  if (rows) {
+    out->rows = reinterpret_cast<float *>(take(D * (L + 2) * sizeof(float)));
+    out->interactions = reinterpret_cast<uint32_t *>(take(D * L * sizeof(uint32_t)));
   }
-  if (temp) cudaFreeAsync(temp, stream);
-  if (idx) cudaFreeAsync(idx, stream);
-  if (keys) cudaFreeAsync(keys, stream);
+  const int grid = 4 * sm_count;
+  record_keys_kernel<<<grid, 256, 0, stream>>>(rec, D, keys, idx);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys, keys + D, idx, idx + D, (int)D, 0,
+                                        kPhotonBits + 5, stream);
+  if (e == cudaSuccess) {
+    gather_kernel<<<grid, 256, 0, stream>>>(idx + D, D, rec, out->records, rows, out->rows, inter,
+                                            out->interactions, L);
+    e = cudaGetLastError();
+  }
   return e;
 }
 
