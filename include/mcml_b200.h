@@ -467,6 +467,20 @@ int mcml_format_rows_text(const float *rows, uint64_t n_rows, uint32_t row_len, 
 int mcml_uniform_stream(int device, uint64_t seed, uint64_t subsequence,
                         uint64_t count, float *out);
 
+/*
+ * Known-answer probes of the walk's own device functions (spin,
+ * transport.cu:742-786; Reflect, transport.cu:790-853), n samples, each
+ * thread on its own XORWOW subsequence of `seed`.  out[2] (host):
+ *   mcml_probe_spin:    mean cos(theta), mean cos^2(theta) of spin() with
+ *                       anisotropy g applied to a photon going along +z;
+ *   mcml_probe_reflect: fraction reflected at an interface n1 -> n2 for
+ *                       incidence cosine cos_i, mean |dz| of the
+ *                       transmitted photons.
+ */
+int mcml_probe_spin(int device, float g, uint64_t n, uint64_t seed, double *out);
+int mcml_probe_reflect(int device, float n1, float n2, float cos_i, uint64_t n, uint64_t seed,
+                       double *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -252,6 +252,9 @@ _SIGNATURES = [
     ("mcml_checkpoint_read_info", C.c_int, [C.c_char_p, C.POINTER(CheckpointInfo)]),
     ("mcml_write_host_outputs", C.c_int, [C.POINTER(Sim), C.POINTER(HostData), C.c_char_p,
                                           C.c_char_p, C.c_uint32, C.c_double, C.c_double]),
+    ("mcml_probe_spin", C.c_int, [C.c_int, C.c_float, C.c_uint64, C.c_uint64, C.c_void_p]),
+    ("mcml_probe_reflect", C.c_int, [C.c_int, C.c_float, C.c_float, C.c_float, C.c_uint64,
+                                     C.c_uint64, C.c_void_p]),
     ("mcml_format_rows_text", C.c_int, [C.c_void_p, C.c_uint64, C.c_uint32, C.c_void_p,
                                         C.c_uint64, C.POINTER(C.c_uint64)]),
 ]
@@ -369,6 +372,23 @@ def format_rows_text(rows: np.ndarray) -> bytes:
     _check(lib.mcml_format_rows_text(rows.ctypes.data, n, rl, buf, size.value, C.byref(size)),
            "mcml_format_rows_text")
     return buf.raw[:size.value]
+
+
+def probe_spin(g: float, n: int, seed: int = 1, device: int = 0) -> tuple[float, float]:
+    """Mean cos and cos^2 of the walk's spin() with anisotropy g (GPU)."""
+    lib = load_library()
+    out = (C.c_double * 2)()
+    _check(lib.mcml_probe_spin(device, g, n, seed, out), "mcml_probe_spin")
+    return out[0], out[1]
+
+
+def probe_reflect(n1: float, n2: float, cos_i: float, n: int, seed: int = 1,
+                  device: int = 0) -> tuple[float, float]:
+    """Reflected fraction and mean transmitted |dz| of the walk's reflect() (GPU)."""
+    lib = load_library()
+    out = (C.c_double * 2)()
+    _check(lib.mcml_probe_reflect(device, n1, n2, cos_i, n, seed, out), "mcml_probe_reflect")
+    return out[0], out[1]
 
 
 def checkpoint_info(path: os.PathLike | str) -> CheckpointInfo:

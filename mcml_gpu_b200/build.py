@@ -31,7 +31,7 @@ NVCC_FLAGS = ARCH + [
 ]
 
 LIB_SOURCES = ["kernels.cu", "capi.cu", "config.cpp", "writers.cpp", "noalloc.cu", "batch.cu",
-               "wmc.cu", "mlp.cu", "checkpoint.cpp", "order.cu"]
+               "wmc.cu", "mlp.cu", "checkpoint.cpp", "order.cu", "probes.cu"]
 HEADERS = ["photon.cuh", "kernels.h", "internal.h", "json_min.h", "params.h"]
 
 

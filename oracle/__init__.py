@@ -58,6 +58,8 @@ def load() -> C.CDLL:
     lib.oracle_replay.argtypes = [vp, C.c_int, C.c_uint64, C.c_uint64, vp, vp, C.c_int, vp, vp,
                                   vp, vp, C.c_uint32, C.c_uint32, C.c_float, C.c_float]
     lib.oracle_replay.restype = C.c_int
+    lib.oracle_energy.argtypes = [vp, C.c_int, C.c_uint64, C.c_uint64, C.c_int, vp]
+    lib.oracle_energy.restype = C.c_int
     _lib = lib
     return lib
 
@@ -143,3 +145,17 @@ def replay(sim, seed: int, ids: np.ndarray, sds: np.ndarray, *, fp64: bool = Fal
     if rc != 0:
         raise RuntimeError("oracle_replay failed")
     return rows, inter, arz, a0z
+
+
+ENERGY_FIELDS = ("start", "absorbed", "top", "bottom", "capped", "roulette_lost",
+                 "roulette_gained", "rounding")
+
+
+def energy(sim, n: int, seed: int, *, fp64: bool = False, roulette: bool = True) -> dict:
+    """Where the start weight of n photons went (weight quanta): see
+    oracle_energy in mcml_oracle.cpp."""
+    lib = load()
+    out = np.zeros(8, np.float64)
+    if lib.oracle_energy(C.byref(sim), int(fp64), seed, n, int(roulette), _p(out)) != 0:
+        raise RuntimeError("oracle_energy failed")
+    return dict(zip(ENERGY_FIELDS, out.tolist()))

@@ -412,6 +412,76 @@ int walk_first(Rng &g, const Tab<R> &t, Detection *det, int *n_det) {
   }
 }
 
+// Energy bookkeeping of one photon's first pass (a known-answer test of
+// the walk's weight arithmetic): every quantum of the start weight ends up
+// absorbed, leaving through the top or the bottom, still held at the step
+// cap, or removed / added by roulette -- up to the rounding of the float
+// weight in `w - w_t`, which is tracked exactly (weights are integers, so
+// each rounding is an integer).  roulette = false replaces the roulette by
+// "live while w > 0" (the step cap still ends every photon).
+struct Energy {
+  double start, absorbed, top, bottom, capped, roulette_lost, roulette_gained, rounding;
+};
+
+template <typename R, typename Rng>
+void walk_energy(Rng &g, const Tab<R> &t, bool roulette, Energy &e) {
+  Ph<R> p;
+  launch(p, g, t);
+  e.start += (double)p.w;
+  for (;;) {
+    R s;
+    const int nl = hop(p, s, g, t);
+    p.steps++;
+    clampz(p, t);
+    if (nl != p.layer) {
+      const int temp_layer = p.layer;
+      s = 0;
+      if (!reflect(p, nl, g, t)) {
+        if (nl == 0) {
+          bool any = false;
+          for (int i = 1; i <= t.n_sds; ++i) {
+            R wd;
+            if (det_hit(p, t, i, wd)) any = true;
+          }
+          if (any || uni<R>(g) > t.det_refl) {
+            e.top += (double)p.w;
+            p.w = 0;
+          } else {
+            p.dz = -p.dz;
+            p.z = -p.z;
+            p.layer = temp_layer;
+          }
+        }
+        if (nl > t.n_layers) {
+          e.bottom += (double)p.w;
+          p.w = 0;
+        }
+      }
+    }
+    if (s > 0) {
+      const double before = (double)p.w;
+      const uint32_t wt = drop(p, t);
+      e.absorbed += (double)wt;
+      e.rounding += (double)p.w - (before - (double)wt);
+      spin(p, t.g[p.layer], g);
+    }
+    if (p.steps >= kMaxScatter) {
+      e.capped += (double)p.w;
+      return;
+    }
+    if (!roulette) {
+      if (p.w == 0) return;
+      continue;
+    }
+    const double before = (double)p.w;
+    if (!survive(p, g, false)) {
+      e.roulette_lost += before;
+      return;
+    }
+    e.roulette_gained += (double)p.w - before;
+  }
+}
+
 struct Grid {
   uint64_t *A_rz = nullptr;  // nz x nr of one SDS (may be null)
   uint64_t *A0_z = nullptr;  // nz of one SDS (may be null)
@@ -677,6 +747,32 @@ int oracle_replay(const mcml_sim *sim, int fp64, uint64_t seed, uint64_t n,
     }
   }
   return bad ? -1 : 0;
+}
+
+// Energy bookkeeping (walk_energy) of photons [0, count) with PCG32
+// streams of `seed`; out: start, absorbed, top, bottom, capped,
+// roulette_lost, roulette_gained, rounding (weight quanta, FP64 sums of
+// integers).  Single-threaded so the sums are exact.
+int oracle_energy(const mcml_sim *sim, int fp64, uint64_t seed, uint64_t count, int roulette,
+                  double *out) {
+  if (!sim || !out) return -1;
+  Energy e{};
+  Tab<float> tf;
+  Tab<double> td;
+  make_tab(*sim, tf);
+  make_tab(*sim, td);
+  for (uint64_t k = 0; k < count; ++k) {
+    Pcg32 g;
+    g.seed(seed, k);
+    if (fp64)
+      walk_energy(g, td, roulette != 0, e);
+    else
+      walk_energy(g, tf, roulette != 0, e);
+  }
+  const double v[8] = {e.start, e.absorbed, e.top, e.bottom, e.capped, e.roulette_lost,
+                       e.roulette_gained, e.rounding};
+  std::memcpy(out, v, sizeof(v));
+  return 0;
 }
 
 }  // extern "C"
