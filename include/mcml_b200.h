@@ -313,7 +313,9 @@ int mcml_wmc_rescale(const mcml_wmc_set *set, const float *base_mua, const float
  * No counterpart in the reference.  An ensemble of MLPs
  * (in -> hidden x depth, GELU -> out) trained and evaluated by this
  * library's BF16 tensor-core kernels with FP32 accumulation and FP32
- * master weights (Adam).  Inputs and targets are normalised with
+ * master weights (Adam): the forward pass on tcgen05 (accumulators in
+ * tensor memory), the backward products on mma.sync.  Limits: in_dim and
+ * hidden at most 256, hidden a multiple of 16, out_dim <= hidden.  Inputs and targets are normalised with
  * mcml_mlp_set_normalization; predictions come back de-normalised with the
  * ensemble's spread.  X, T, mean and spread are DEVICE arrays.
  */
@@ -329,7 +331,7 @@ int mcml_mlp_set_normalization(mcml_mlp *mlp, const float *x_mean, const float *
                                const float *t_mean, const float *t_std);
 int64_t mcml_mlp_num_params(const mcml_mlp *mlp);
 /* FP32 parameters of one member (host), layer by layer: W (fan_in x
- * fan_out, row-major, fan_in of layer 0 padded to a multiple of 8) then b. */
+ * fan_out, row-major, fan_in of layer 0 padded to a multiple of 16) then b. */
 int mcml_mlp_get_params(mcml_mlp *mlp, float *host, int member);
 int mcml_mlp_set_params(mcml_mlp *mlp, const float *host, int member);
 /* Loss and gradients of every member on rows [0, n) (no update; host out). */

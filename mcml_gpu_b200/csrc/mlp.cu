@@ -6,12 +6,13 @@
 // Weights are kept in FP32 (master copy, Adam state) and mirrored to BF16
 // for the tensor-core GEMMs, which accumulate in FP32.
 //
-// GEMM: C[M x N] = op(A)[M x K] * op(B)[K x N], BF16 operands staged in
+// Forward: tc_layer_kernel, one 128-row tile per CTA on the tcgen05
+// tensor cores (operands in shared memory, FP32 accumulator in tensor
+// memory, bias + GELU epilogue from tcgen05.ld).
+//
+// Backward GEMM: C[M x N] = op(A)[M x K] * op(B)[K x N], BF16 operands staged in
 // shared memory, mma.sync m16n8k16 fragments loaded with ldmatrix, FP32
 // accumulators, and a fused epilogue:
-//   kBiasGelu : Z = acc + bias (kept in FP32 for the backward pass),
-//               H = bf16(gelu(Z))
-//   kBias     : Y = acc + bias (FP32; the output layer)
 //   kGeluBack : dZ = bf16(acc * gelu'(Zprev))   (back through an activation)
 //   kStoreF32 : G = acc (FP32; weight gradients)
 // op(A) = A or A^T, op(B) = B or B^T by template flags, which gives the
@@ -39,7 +40,7 @@ constexpr int BM = 64, BN = 64, BK = 32;  // CTA tile
 constexpr int kGemmThreads = 128;         // 4 warps, 2 x 2, warp tile 32 x 32
 constexpr int PAD = 8;                    // smem row padding (bf16 elements)
 
-enum Epi { kBiasGelu = 0, kBias = 1, kGeluBack = 2, kStoreF32 = 3 };
+enum Epi { kGeluBack = 2, kStoreF32 = 3 };
 
 __device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
 __device__ __forceinline__ float gelu_grad(float z) {
@@ -58,11 +59,11 @@ struct GemmArgs {
   long long lda, strideA;  // per-member strides (elements)
   const bf16 *B;
   long long ldb, strideB;
-  const float *bias;       // [N] per member (kBiasGelu, kBias)
+  const float *bias;       // unused by the backward epilogues
   long long strideBias;
-  float *outF;             // FP32 output (Z for kBiasGelu, Y, G)
+  float *outF;             // FP32 output (weight gradients G)
   long long ldo, strideO;
-  bf16 *outH;              // BF16 output (H for kBiasGelu, dZ for kGeluBack)
+  bf16 *outH;              // BF16 output (dZ for kGeluBack)
   long long ldh, strideH;
   const float *aux;        // Zprev for kGeluBack
   long long ldx, strideX;
@@ -140,7 +141,6 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(const GemmArgs g) {
   }
 
   // Epilogue: thread holds rows (lane>>2) and (lane>>2)+8, columns 2*(lane&3)+{0,1}.
-  const float *bias = g.bias ? g.bias + z * g.strideBias : nullptr;
 #pragma unroll
   for (int i = 0; i < 2; ++i)
 #pragma unroll
@@ -151,17 +151,11 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(const GemmArgs g) {
         const int n = n0 + wn + j * 8 + 2 * (lane & 3) + (r & 1);
         if (m >= g.M || n >= g.N) continue;
         const float v = acc[i][j][r];
-        if (EPI == kBiasGelu) {
-          const float zz = v + bias[n];
-          g.outF[z * g.strideO + (long long)m * g.ldo + n] = zz;
-          g.outH[z * g.strideH + (long long)m * g.ldh + n] = __float2bfloat16(gelu(zz));
-        } else if (EPI == kBias) {
-          g.outF[z * g.strideO + (long long)m * g.ldo + n] = v + bias[n];
-        } else if (EPI == kGeluBack) {
+        if (EPI == kStoreF32) {
+          g.outF[z * g.strideO + (long long)m * g.ldo + n] = v;
+        } else {  // kGeluBack
           const float zp = g.aux[z * g.strideX + (long long)m * g.ldx + n];
           g.outH[z * g.strideH + (long long)m * g.ldh + n] = __float2bfloat16(v * gelu_grad(zp));
-        } else {
-          g.outF[z * g.strideO + (long long)m * g.ldo + n] = v;
         }
       }
 }
@@ -170,6 +164,235 @@ template <bool TA, bool TB, int EPI>
 cudaError_t gemm(const GemmArgs &g, int members, cudaStream_t s) {
   dim3 grid((g.N + BN - 1) / BN, (g.M + BM - 1) / BM, members);
   gemm_kernel<TA, TB, EPI><<<grid, kGemmThreads, 0, s>>>(g);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Forward layer on the 5th-generation tensor cores (tcgen05):
+//   C[M x N] = A[M x K] * W[K x N] (+ bias, epilogue), one 128-row tile per CTA.
+// A (activations, row-major) is staged in shared memory K-major, W
+// (row-major, fan_in x fan_out) MN-major, both in the no-swizzle
+// core-matrix layout (8 rows x 16 bytes per core matrix):
+//   A: element (r, k) at (k/8)*kLboA + (r/8)*128 + (r%8)*16 + (k%8)*2
+//   W: element (k, n) at (k/8)*LboB  + (n/8)*128 + (k%8)*16 + (n%8)*2
+// so the descriptors carry SBO = 128 bytes (next 8 rows / 8 columns) and
+// LBO = the distance between K groups of 8.  One thread issues the K/16
+// MMAs (M = 128, N <= 256, BF16 in, FP32 accumulator in tensor memory),
+// commits them to an mbarrier, and all eight warps read the accumulator
+// back with tcgen05.ld (warp w: TMEM lanes 32*(w%4).., column half w/4)
+// for the bias + GELU epilogue.  Every wait is bounded; a timeout sets
+// *status and the tile is skipped.
+constexpr int TCM = 128;            // rows per tile (UMMA M)
+constexpr int kTcThreads = 256;     // 8 warps
+constexpr int kLboA = (TCM / 8) * 128;
+constexpr long long kTcSpin = 1ll << 22;
+
+enum TcEpi { kTcBiasGelu = 0, kTcBias = 1 };
+
+struct TcArgs {
+  int M, N, K, n_valid;     // N: MMA width (multiple of 16); n_valid <= N real columns
+  const bf16 *A;            // M x K, row-major, lda
+  long long lda, strideA;
+  const bf16 *W;            // K x n_valid, row-major (ldw = n_valid)
+  long long strideW;
+  const float *bias;
+  long long strideBias;
+  float *Z;                 // kTcBiasGelu: pre-activations (may be null); kTcBias: output
+  long long ldz, strideZ;
+  bf16 *H;                  // kTcBiasGelu: activations
+  long long ldh, strideH;
+  unsigned *status;
+};
+
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version (Blackwell)
+  return d;                // base offset 0, no swizzle
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
+  for (long long i = 0; i < kTcSpin; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred P;\n mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, P;\n}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(phase)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+template <int EPI>
+__global__ void __launch_bounds__(kTcThreads, 1) tc_layer_kernel(const TcArgs g) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int z = blockIdx.z;
+  const int m0 = blockIdx.x * TCM;
+  const int K = g.K, N = g.N;
+  const uint32_t lboB = (uint32_t)(N / 8) * 128;
+  unsigned char *sA = smem;
+  unsigned char *sB = smem + (size_t)TCM * K * 2;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sB + (size_t)K * N * 2);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 1);
+  const uint32_t sA_u = smem_u32(sA), sB_u = smem_u32(sB), bar_u = smem_u32(bar);
+  const uint32_t ncols = N <= 32 ? 32 : (N <= 64 ? 64 : (N <= 128 ? 128 : 256));
+
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar_u) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                     smem_u32(tslot)),
+                 "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+
+  // Operands into shared memory.  A: 16-byte copies, rows past M zero-filled.
+  const bf16 *A = g.A + z * g.strideA;
+  const int kc8 = K / 8;
+  for (int c = tid; c < TCM * kc8; c += kTcThreads) {
+    const int r_lo = c & 7, rest = c >> 3;
+    const int kc = rest % kc8, r = (rest / kc8) * 8 + r_lo;
+    const uint32_t dst = sA_u + kc * kLboA + (r >> 3) * 128 + r_lo * 16;
+    const int gr = m0 + r;
+    const bf16 *src = A + (long long)(gr < g.M ? gr : 0) * g.lda + kc * 8;
+    const uint32_t bytes = gr < g.M ? 16u : 0u;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(bytes)
+                 : "memory");
+  }
+  const bf16 *W = g.W + z * g.strideW;
+  if (g.n_valid == N) {
+    // W rows of N values: 16-byte copies, k % 8 fastest (one core matrix per 8 lanes)
+    const int nc8 = N / 8;
+    for (int c = tid; c < K * nc8; c += kTcThreads) {
+      const int k_lo = c & 7, rest = c >> 3;
+      const int nc = rest % nc8, k = (rest / nc8) * 8 + k_lo;
+      const uint32_t dst = sB_u + (k >> 3) * lboB + nc * 128 + k_lo * 16;
+      const bf16 *src = W + (long long)k * N + nc * 8;
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
+    }
+  } else {
+    // narrow output layer: element copies, columns past n_valid zero
+    bf16 *sb = reinterpret_cast<bf16 *>(sB);
+    for (int e = tid; e < K * N; e += kTcThreads) {
+      const int k = e / N, n = e % N;
+      const bf16 v = n < g.n_valid ? W[(long long)k * g.n_valid + n] : __float2bfloat16(0.0f);
+      sb[((k >> 3) * lboB + (n >> 3) * 128 + (k & 7) * 16 + (n & 7) * 2) / 2] = v;
+    }
+  }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t tmem = *tslot;
+
+  if (tid == 0) {
+    const uint32_t idesc = (1u << 4)                     // D: FP32
+                           | (1u << 7) | (1u << 10)      // A, B: BF16
+                           | (0u << 15) | (1u << 16)     // A K-major, B MN-major
+                           | ((uint32_t)(N >> 3) << 17)  // N
+                           | ((uint32_t)(TCM >> 4) << 24);  // M
+    for (int j = 0; j < K / 16; ++j) {
+      const uint64_t ad = umma_desc(sA_u + 2 * j * kLboA, kLboA, 128);
+      const uint64_t bd = umma_desc(sB_u + 2 * j * lboB, lboB, 128);
+      const uint32_t acc = j > 0 ? 1u : 0u;
+      asm volatile(
+          "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+          " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+          "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+          : "memory");
+    }
+    asm volatile(
+        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+            bar_u)
+        : "memory");
+  }
+  bool ok = mbar_wait(bar_u, 0);
+  if (!ok) {
+    atomicOr(g.status, 1u);
+    mbar_wait(bar_u, 0);  // a second bounded chance for the MMAs before the memory is freed
+  }
+  ok = __syncthreads_and(ok) != 0;  // the epilogue's tcgen05.ld needs whole warps
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+
+  if (ok) {
+    const int q = warp & 3, half = warp >> 2;
+    const int row = m0 + q * 32 + lane;
+    const int c_begin = half * (N / 2), c_end = c_begin + N / 2;
+    const float *bias = g.bias + z * g.strideBias;
+    for (int c0 = c_begin; c0 < c_end; c0 += 8) {
+      uint32_t v[8];
+      const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0;
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+            "=r"(v[7])
+          : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+      if (row >= g.M) continue;
+      float f[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) f[i] = __uint_as_float(v[i]) + (c0 + i < g.n_valid ? bias[c0 + i] : 0.0f);
+      if (EPI == kTcBiasGelu) {
+        if (g.Z) {
+          float4 *zp = reinterpret_cast<float4 *>(g.Z + z * g.strideZ + (long long)row * g.ldz + c0);
+          zp[0] = make_float4(f[0], f[1], f[2], f[3]);
+          zp[1] = make_float4(f[4], f[5], f[6], f[7]);
+        }
+        __align__(16) bf16 h[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) h[i] = __float2bfloat16(gelu(f[i]));
+        *reinterpret_cast<uint4 *>(g.H + z * g.strideH + (long long)row * g.ldh + c0) =
+            *reinterpret_cast<const uint4 *>(h);
+      } else {
+        float *y = g.Z + z * g.strideZ + (long long)row * g.ldz;
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+          if (c0 + i < g.n_valid) y[c0 + i] = f[i];
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem),
+                 "r"(ncols)
+                 : "memory");
+}
+
+size_t tc_smem_bytes(int K, int N) {
+  // operands + mbarrier + TMEM slot; at least 120 KB so that one CTA runs
+  // per SM and its tensor-memory allocation never waits for another's
+  const size_t need = (size_t)TCM * K * 2 + (size_t)K * N * 2 + 16;
+  return std::max<size_t>(need, 120 * 1024);
+}
+
+template <int EPI>
+cudaError_t tc_layer(const TcArgs &g, int members, cudaStream_t s) {
+  if (g.N % 16 || g.N < 16 || g.N > 256 || g.K % 16 || g.K < 16 || g.K > 256 || g.n_valid > g.N)
+    return cudaErrorInvalidValue;
+  const size_t smem = tc_smem_bytes(g.K, g.N);
+  static bool configured[64] = {};  // per device: the attribute is per context
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  if (!configured[dev]) {
+    e = cudaFuncSetAttribute(tc_layer_kernel<EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             200 * 1024);
+    if (e != cudaSuccess) return e;
+    configured[dev] = true;
+  }
+  dim3 grid((g.M + TCM - 1) / TCM, 1, members);
+  tc_layer_kernel<EPI><<<grid, kTcThreads, smem, s>>>(g);
   return cudaGetLastError();
 }
 
@@ -286,7 +509,9 @@ struct mcml_mlp {
   std::vector<int> fan_in, fan_out;
   std::vector<long long> w_off, b_off;  // offsets into the per-member parameter block
   long long per_member = 0;        // parameters per member
-  float *d_w = nullptr;            // E x per_member FP32 master (weights then biases per layer)
+  long long stride = 0;            // per_member rounded up to 8 (16-byte aligned BF16 blocks)
+  unsigned *d_status = nullptr;    // tensor-core kernel timeouts
+  float *d_w = nullptr;            // E x stride FP32 master (weights then biases per layer)
   float *d_m = nullptr, *d_v = nullptr, *d_g = nullptr;
   bf16 *d_w16 = nullptr;           // BF16 mirror (same layout)
   float *d_xmean = nullptr, *d_xinv = nullptr, *d_tmean = nullptr, *d_tinv = nullptr,
@@ -303,6 +528,8 @@ struct mcml_mlp {
   bf16 *d_dh = nullptr;            // E x cap x hidden
   uint32_t *d_idx = nullptr;       // E x cap
   float *d_loss = nullptr;         // E
+  uint32_t *d_perm = nullptr;      // E x n: one epoch's shuffles
+  size_t perm_cap = 0;
 
   ~mcml_mlp() {
     int prev = -1;
@@ -313,6 +540,8 @@ struct mcml_mlp {
     dfree(d_xmean); dfree(d_xinv); dfree(d_tmean); dfree(d_tinv); dfree(d_tstd);
     dfree(d_x); dfree(d_z); dfree(d_h); dfree(d_y); dfree(d_dy); dfree(d_dh); dfree(d_idx);
     dfree(d_loss);
+    dfree(d_perm);
+    dfree(d_status);
     if (own_stream && stream) cudaStreamDestroy(stream);
     if (prev >= 0 && prev != device) cudaSetDevice(prev);
   }
@@ -348,15 +577,18 @@ int ensure_cap(mcml_mlp *p, int rows) {
   return MCML_OK;
 }
 
-// Forward of all members on rows [0, n) already gathered into d_x.
-int forward(mcml_mlp *p, int n) {
-  const long long H = p->hidden, cap = p->cap, P = p->per_member;
+// Forward of all members on rows [0, n) already gathered into d_x, on the
+// tensor cores (tc_layer_kernel): hidden layers keep Z (FP32) for the
+// backward pass and H (BF16) for the next layer; the output layer writes Y.
+int forward(mcml_mlp *p, int n, bool keep_z) {
+  const long long H = p->hidden, cap = p->cap, P = p->stride, D = p->depth;
   for (int l = 0; l < p->layers; ++l) {
-    GemmArgs g;
+    TcArgs g;
     std::memset(&g, 0, sizeof(g));
     g.M = n;
-    g.N = p->fan_out[l];
     g.K = l == 0 ? p->in_pad : (int)H;
+    g.n_valid = p->fan_out[l];
+    g.N = (p->fan_out[l] + 15) / 16 * 16;
     if (l == 0) {
       g.A = p->d_x;
       g.lda = p->in_pad;
@@ -364,34 +596,46 @@ int forward(mcml_mlp *p, int n) {
     } else {
       g.A = p->d_h + (long long)(l - 1) * cap * H;
       g.lda = H;
-      g.strideA = (long long)p->depth * cap * H;
+      g.strideA = D * cap * H;
     }
-    g.B = p->d_w16 + p->w_off[l];
-    g.ldb = p->fan_out[l];
-    g.strideB = P;
+    g.W = p->d_w16 + p->w_off[l];
+    g.strideW = P;
     g.bias = p->d_w + p->b_off[l];
     g.strideBias = P;
+    g.status = p->d_status;
     if (l < p->depth) {
-      g.outF = p->d_z + (long long)l * cap * H;
-      g.ldo = H;
-      g.strideO = (long long)p->depth * cap * H;
-      g.outH = p->d_h + (long long)l * cap * H;
+      g.Z = keep_z ? p->d_z + (long long)l * cap * H : nullptr;
+      g.ldz = H;
+      g.strideZ = D * cap * H;
+      g.H = p->d_h + (long long)l * cap * H;
       g.ldh = H;
-      g.strideH = (long long)p->depth * cap * H;
-      MLP_TRY((gemm<false, false, kBiasGelu>(g, p->E, p->stream)));
+      g.strideH = D * cap * H;
+      MLP_TRY(tc_layer<kTcBiasGelu>(g, p->E, p->stream));
     } else {
-      g.outF = p->d_y;
-      g.ldo = p->out_dim;
-      g.strideO = cap * p->out_dim;
-      MLP_TRY((gemm<false, false, kBias>(g, p->E, p->stream)));
+      g.Z = p->d_y;
+      g.ldz = p->out_dim;
+      g.strideZ = cap * p->out_dim;
+      MLP_TRY(tc_layer<kTcBias>(g, p->E, p->stream));
     }
+  }
+  return MCML_OK;
+}
+
+// Tensor-core kernel timeouts seen so far (then cleared): MCML_E_BUDGET.
+int check_status(mcml_mlp *p) {
+  unsigned st = 0;
+  MLP_TRY(cudaMemcpyAsync(&st, p->d_status, sizeof(st), cudaMemcpyDeviceToHost, p->stream));
+  MLP_TRY(cudaStreamSynchronize(p->stream));
+  if (st) {
+    MLP_TRY(cudaMemset(p->d_status, 0, sizeof(unsigned)));
+    return set_error(MCML_E_BUDGET, "a tensor-core MMA did not complete in time");
   }
   return MCML_OK;
 }
 
 // Backward from dY (in d_dy, BF16) to all weight/bias gradients in d_g.
 int backward(mcml_mlp *p, int n) {
-  const long long H = p->hidden, cap = p->cap, P = p->per_member, D = p->depth;
+  const long long H = p->hidden, cap = p->cap, P = p->stride, D = p->depth;
   bf16 *dcur = p->d_dy;   // gradient w.r.t. the current layer's output (pre-activation)
   bf16 *dnext = p->d_dh;
   long long dcur_ld = p->out_dim;
@@ -457,15 +701,18 @@ int mcml_mlp_create(const mcml_mlp_config *cfg, mcml_mlp **out) {
   clear_error();
   if (!cfg || !out) return set_error(MCML_E_INVALID, "mcml_mlp_create: null argument");
   *out = nullptr;
+  // The tensor-core forward takes K <= 256 and N <= 256 in multiples of 16.
   if (cfg->in_dim < 1 || cfg->hidden < 16 || cfg->depth < 1 || cfg->out_dim < 1 ||
-      cfg->ensemble < 1 || cfg->in_dim > 4096 || cfg->hidden > 4096 ||
+      cfg->ensemble < 1 || cfg->in_dim > 256 || cfg->hidden > 256 || cfg->hidden % 16 != 0 ||
       cfg->out_dim > cfg->hidden)
-    return set_error(MCML_E_INVALID, "mcml_mlp_create: bad dimensions");
+    return set_error(MCML_E_INVALID,
+                     "mcml_mlp_create: bad dimensions (in_dim <= 256; hidden a multiple of 16, "
+                     "at most 256; out_dim <= hidden)");
   std::unique_ptr<mcml_mlp> p(new mcml_mlp());
   p->device = cfg->device;
   MlpGuard gd(cfg->device);
   p->in_dim = cfg->in_dim;
-  p->in_pad = (cfg->in_dim + 7) / 8 * 8;
+  p->in_pad = (cfg->in_dim + 15) / 16 * 16;
   p->hidden = cfg->hidden;
   p->depth = cfg->depth;
   p->out_dim = cfg->out_dim;
@@ -483,7 +730,8 @@ int mcml_mlp_create(const mcml_mlp_config *cfg, mcml_mlp **out) {
     off += fo;
   }
   p->per_member = off;
-  const long long total = off * p->E;
+  p->stride = (off + 7) / 8 * 8;
+  const long long total = p->stride * p->E;
   if (cfg->stream) {
     p->stream = (cudaStream_t)cfg->stream;
   } else {
@@ -501,6 +749,8 @@ int mcml_mlp_create(const mcml_mlp_config *cfg, mcml_mlp **out) {
   MLP_TRY(cudaMalloc(&p->d_tinv, p->out_dim * sizeof(float)));
   MLP_TRY(cudaMalloc(&p->d_tstd, p->out_dim * sizeof(float)));
   MLP_TRY(cudaMalloc(&p->d_loss, p->E * sizeof(float)));
+  MLP_TRY(cudaMalloc(&p->d_status, sizeof(unsigned)));
+  MLP_TRY(cudaMemset(p->d_status, 0, sizeof(unsigned)));
   // He-uniform weights (per member seed), zero biases; the padded input
   // rows of the first matrix are zero.
   std::vector<float> w(total, 0.0f);
@@ -511,7 +761,7 @@ int mcml_mlp_create(const mcml_mlp_config *cfg, mcml_mlp **out) {
       const int real_in = l == 0 ? p->in_dim : fi;
       const float lim = std::sqrt(6.0f / (float)real_in) * (l == p->depth ? 0.5f : 1.0f);
       std::uniform_real_distribution<float> U(-lim, lim);
-      float *W = w.data() + (long long)e * p->per_member + p->w_off[l];
+      float *W = w.data() + (long long)e * p->stride + p->w_off[l];
       for (int i = 0; i < fi; ++i)
         for (int j = 0; j < fo; ++j) W[(long long)i * fo + j] = i < real_in ? U(rng) : 0.0f;
     }
@@ -567,7 +817,7 @@ int mcml_mlp_get_params(mcml_mlp *p, float *host, int member) {
   if (!p || !host || member < 0 || member >= p->E) return set_error(MCML_E_INVALID, "bad argument");
   MlpGuard gd(p->device);
   MLP_TRY(cudaStreamSynchronize(p->stream));
-  MLP_TRY(cudaMemcpy(host, p->d_w + (long long)member * p->per_member, p->per_member * sizeof(float),
+  MLP_TRY(cudaMemcpy(host, p->d_w + (long long)member * p->stride, p->per_member * sizeof(float),
                      cudaMemcpyDeviceToHost));
   return MCML_OK;
 }
@@ -576,10 +826,10 @@ int mcml_mlp_set_params(mcml_mlp *p, const float *host, int member) {
   clear_error();
   if (!p || !host || member < 0 || member >= p->E) return set_error(MCML_E_INVALID, "bad argument");
   MlpGuard gd(p->device);
-  float *dst = p->d_w + (long long)member * p->per_member;
+  float *dst = p->d_w + (long long)member * p->stride;
   MLP_TRY(cudaMemcpy(dst, host, p->per_member * sizeof(float), cudaMemcpyHostToDevice));
   to_bf16_kernel<<<(unsigned)((p->per_member + 255) / 256), 256, 0, p->stream>>>(
-      dst, p->d_w16 + (long long)member * p->per_member, p->per_member);
+      dst, p->d_w16 + (long long)member * p->stride, p->per_member);
   MLP_TRY(cudaGetLastError());
   MLP_TRY(cudaStreamSynchronize(p->stream));
   return MCML_OK;
@@ -603,7 +853,7 @@ int mcml_mlp_gradients(mcml_mlp *p, const float *X, const float *T, int n, float
   gather_x_kernel<<<dim3((unsigned)((n * p->in_pad + 255) / 256), 1, p->E), 256, 0, p->stream>>>(
       X, p->d_idx, n, p->in_dim, p->in_pad, p->d_xmean, p->d_xinv, cap, p->d_x, cap * p->in_pad);
   MLP_TRY(cudaGetLastError());
-  rc = forward(p, n);
+  rc = forward(p, n, true);
   if (rc) return rc;
   MLP_TRY(cudaMemsetAsync(p->d_loss, 0, p->E * sizeof(float), p->stream));
   loss_grad_kernel<<<dim3((unsigned)((n * p->out_dim + 255) / 256), 1, p->E), 256, 0, p->stream>>>(
@@ -612,11 +862,13 @@ int mcml_mlp_gradients(mcml_mlp *p, const float *X, const float *T, int n, float
   MLP_TRY(cudaGetLastError());
   rc = backward(p, n);
   if (rc) return rc;
-  MLP_TRY(cudaStreamSynchronize(p->stream));
+  rc = check_status(p);
+  if (rc) return rc;
   if (loss_out) MLP_TRY(cudaMemcpy(loss_out, p->d_loss, p->E * sizeof(float), cudaMemcpyDeviceToHost));
   if (grads_out)
-    MLP_TRY(cudaMemcpy(grads_out, p->d_g, (size_t)p->E * p->per_member * sizeof(float),
-                       cudaMemcpyDeviceToHost));
+    MLP_TRY(cudaMemcpy2D(grads_out, p->per_member * sizeof(float), p->d_g,
+                         p->stride * sizeof(float), p->per_member * sizeof(float), p->E,
+                         cudaMemcpyDeviceToHost));
   return MCML_OK;
 }
 
@@ -627,36 +879,43 @@ int mcml_mlp_train_epoch(mcml_mlp *p, const float *X, const float *T, uint64_t n
                          float lr, uint64_t shuffle_seed, float *loss_out) {
   clear_error();
   if (!p || !X || !T || n < 1 || batch < 1) return set_error(MCML_E_INVALID, "bad argument");
+  if (n >= (1ull << 32)) return set_error(MCML_E_INVALID, "at most 2^32 - 1 rows");
   MlpGuard gd(p->device);
-  int rc = ensure_cap(p, (int)batch);
+  int rc = ensure_cap(p, (int)std::min<uint64_t>(batch, n));
   if (rc) return rc;
   const long long cap = p->cap;
-  std::vector<std::vector<uint32_t>> perm(p->E, std::vector<uint32_t>(n));
+  // The epoch's shuffles (one per member) go to the device in one copy;
+  // minibatches index into them, so the loop below never waits for the host.
+  std::vector<uint32_t> perm((size_t)p->E * n);
   for (int e = 0; e < p->E; ++e) {
-    for (uint64_t i = 0; i < n; ++i) perm[e][i] = (uint32_t)i;
+    uint32_t *pe = &perm[(size_t)e * n];
+    for (uint64_t i = 0; i < n; ++i) pe[i] = (uint32_t)i;
     std::mt19937_64 rng(shuffle_seed * 7919ull + (uint64_t)e);
-    std::shuffle(perm[e].begin(), perm[e].end(), rng);
+    std::shuffle(pe, pe + n, rng);
   }
-  std::vector<uint32_t> idx((size_t)p->E * cap);
-  std::vector<double> loss_sum(p->E, 0.0);
-  std::vector<float> loss(p->E);
+  if (perm.size() > p->perm_cap) {
+    dfree(p->d_perm);
+    p->perm_cap = 0;
+    MLP_TRY(cudaMalloc(&p->d_perm, perm.size() * sizeof(uint32_t)));
+    p->perm_cap = perm.size();
+  }
+  MLP_TRY(cudaMemcpyAsync(p->d_perm, perm.data(), perm.size() * sizeof(uint32_t),
+                          cudaMemcpyHostToDevice, p->stream));
+  // d_loss sums the minibatch means over the epoch
+  MLP_TRY(cudaMemsetAsync(p->d_loss, 0, p->E * sizeof(float), p->stream));
   uint64_t steps = 0;
-  const long long total = p->per_member * p->E;
+  const long long total = p->stride * p->E;
   for (uint64_t b0 = 0; b0 + batch <= n || (b0 < n && steps == 0); b0 += batch) {
     const int rows = (int)std::min<uint64_t>(batch, n - b0);
-    for (int e = 0; e < p->E; ++e)
-      std::memcpy(&idx[(size_t)e * cap], &perm[e][b0], rows * sizeof(uint32_t));
-    MLP_TRY(cudaMemcpyAsync(p->d_idx, idx.data(), idx.size() * sizeof(uint32_t),
-                            cudaMemcpyHostToDevice, p->stream));
     gather_x_kernel<<<dim3((unsigned)((rows * p->in_pad + 255) / 256), 1, p->E), 256, 0, p->stream>>>(
-        X, p->d_idx, rows, p->in_dim, p->in_pad, p->d_xmean, p->d_xinv, cap, p->d_x, cap * p->in_pad);
+        X, p->d_perm + b0, rows, p->in_dim, p->in_pad, p->d_xmean, p->d_xinv, (long long)n, p->d_x,
+        cap * p->in_pad);
     MLP_TRY(cudaGetLastError());
-    rc = forward(p, rows);
+    rc = forward(p, rows, true);
     if (rc) return rc;
-    MLP_TRY(cudaMemsetAsync(p->d_loss, 0, p->E * sizeof(float), p->stream));
     loss_grad_kernel<<<dim3((unsigned)((rows * p->out_dim + 255) / 256), 1, p->E), 256, 0, p->stream>>>(
-        p->d_y, cap * p->out_dim, T, p->d_idx, cap, rows, p->out_dim, p->d_tmean, p->d_tinv,
-        p->d_dy, cap * std::max(p->hidden, p->out_dim), p->d_loss);
+        p->d_y, cap * p->out_dim, T, p->d_perm + b0, (long long)n, rows, p->out_dim, p->d_tmean,
+        p->d_tinv, p->d_dy, cap * std::max(p->hidden, p->out_dim), p->d_loss);
     MLP_TRY(cudaGetLastError());
     rc = backward(p, rows);
     if (rc) return rc;
@@ -666,15 +925,16 @@ int mcml_mlp_train_epoch(mcml_mlp *p, const float *X, const float *T, uint64_t n
     adam_kernel<<<(unsigned)((total + 255) / 256), 256, 0, p->stream>>>(
         p->d_w, p->d_g, p->d_m, p->d_v, p->d_w16, total, lr, b1, b2, 1e-8f, c1, c2);
     MLP_TRY(cudaGetLastError());
-    MLP_TRY(cudaMemcpyAsync(loss.data(), p->d_loss, p->E * sizeof(float), cudaMemcpyDeviceToHost,
-                            p->stream));
-    MLP_TRY(cudaStreamSynchronize(p->stream));
-    for (int e = 0; e < p->E; ++e) loss_sum[e] += loss[e];
     ++steps;
     if (rows < (int)batch) break;
   }
+  std::vector<float> loss(p->E);
+  MLP_TRY(cudaMemcpyAsync(loss.data(), p->d_loss, p->E * sizeof(float), cudaMemcpyDeviceToHost,
+                          p->stream));
+  rc = check_status(p);
+  if (rc) return rc;
   if (loss_out)
-    for (int e = 0; e < p->E; ++e) loss_out[e] = (float)(loss_sum[e] / (double)steps);
+    for (int e = 0; e < p->E; ++e) loss_out[e] = loss[e] / (float)steps;
   return MCML_OK;
 }
 
@@ -695,7 +955,7 @@ int mcml_mlp_predict(mcml_mlp *p, const float *X, uint64_t n, float *mean, float
         X + r0 * p->in_dim, nullptr, rows, p->in_dim, p->in_pad, p->d_xmean, p->d_xinv, 0, p->d_x,
         cap * p->in_pad);
     MLP_TRY(cudaGetLastError());
-    rc = forward(p, rows);
+    rc = forward(p, rows, false);
     if (rc) return rc;
     ensemble_kernel<<<(unsigned)(((long long)rows * p->out_dim + 255) / 256), 256, 0, p->stream>>>(
         p->d_y, cap * p->out_dim, p->E, (long long)rows * p->out_dim, p->d_tmean, p->d_tstd,
@@ -710,7 +970,7 @@ int mcml_mlp_sync(mcml_mlp *p) {
   if (!p) return set_error(MCML_E_INVALID, "null mlp");
   MlpGuard gd(p->device);
   MLP_TRY(cudaStreamSynchronize(p->stream));
-  return MCML_OK;
+  return check_status(p);
 }
 
 void mcml_mlp_destroy(mcml_mlp *p) { delete p; }

@@ -85,7 +85,7 @@ class MLP:
         self.num_params = int(self.lib.mcml_mlp_num_params(self._h))
 
     def layer_shapes(self):
-        in_pad = (self.in_dim + 7) // 8 * 8
+        in_pad = (self.in_dim + 15) // 16 * 16
         fans = [in_pad] + [self.hidden] * self.depth + [self.out_dim]
         return list(zip(fans[:-1], fans[1:]))
 

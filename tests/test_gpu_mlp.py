@@ -103,3 +103,43 @@ def test_ensemble_learns_smooth_map(gpu_available):
     err = np.abs(mean.cpu().numpy() - T[:4096])
     assert float(np.mean(err)) < 0.05 * float(np.std(T)) * 4
     assert spread.shape == mean.shape and bool(torch.all(spread >= 0))
+
+
+def cpu_forward(params, shapes, X, xm, xs, tm, ts):
+    n, in_dim = X.shape
+    xn = np.zeros((n, shapes[0][0]))
+    inv = np.where(xs > 0, 1.0 / np.where(xs > 0, xs, 1), 0.0)
+    xn[:, :in_dim] = (X - xm) * inv
+    h = bf(xn)
+    off = 0
+    for l, (fi, fo) in enumerate(shapes):
+        W = torch.as_tensor(params[off:off + fi * fo].reshape(fi, fo), dtype=torch.float64)
+        off += fi * fo
+        b = torch.as_tensor(params[off:off + fo], dtype=torch.float64)
+        off += fo
+        z = h @ bf(W) + b
+        h = bf(gelu(z)) if l < len(shapes) - 1 else z
+    return h.numpy() * ts + tm
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("hidden,depth,n", [(256, 4, 300), (64, 3, 129), (128, 2, 1000)])
+def test_tensor_core_forward_matches_cpu_reference(hidden, depth, n, gpu_available):
+    """predict() runs the tcgen05 forward: ensemble mean and spread against
+    a float64 CPU forward that rounds to bf16 where the kernel does (GEMM
+    inputs).  Rows past a 128-row tile boundary and partial tiles included.
+    Tolerance: 1e-2 of the targets' scale (a bf16 rounding of an
+    activation can land on the other side of a boundary)."""
+    rng = np.random.default_rng(7)
+    X = rng.normal(size=(n, 25)).astype(np.float32)
+    T = rng.normal(size=(n, 3)).astype(np.float32) * 2 + 1
+    mlp = sg.MLP(25, 3, hidden=hidden, depth=depth, ensemble=2, seed=3)
+    xm, xs, tm, ts = X.mean(0), X.std(0), T.mean(0), T.std(0)
+    mlp.set_normalization(xm, xs, tm, ts)
+    dev = torch.device("cuda", 0)
+    mean, spread = mlp.predict(torch.from_numpy(X).to(dev))
+    ys = np.stack([cpu_forward(mlp.params(e), mlp.layer_shapes(), X, xm, xs, tm, ts)
+                   for e in range(2)])
+    scale = float(np.abs(ys).mean())
+    assert np.max(np.abs(mean.cpu().numpy() - ys.mean(0))) < 1e-2 * scale
+    assert np.max(np.abs(spread.cpu().numpy() - ys.std(0))) < 1e-2 * scale
