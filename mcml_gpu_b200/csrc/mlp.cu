@@ -42,11 +42,23 @@ constexpr int PAD = 8;                    // smem row padding (bf16 elements)
 
 enum Epi { kGeluBack = 2, kStoreF32 = 3 };
 
-__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+// GELU in its tanh form, 0.5 z (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3))),
+// with the hardware tanh (tanh.approx.f32, relative error ~2^-11, below
+// the bf16 rounding of the activations): a handful of instructions instead
+// of an erf evaluation, in the epilogue that bounds the forward kernel.
+__device__ __forceinline__ float tanh_hw(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float gelu(float z) {
+  const float t = tanh_hw(0.7978845608f * fmaf(0.044715f * z, z * z, z));
+  return fmaf(0.5f * z, t, 0.5f * z);
+}
 __device__ __forceinline__ float gelu_grad(float z) {
-  const float cdf = 0.5f * (1.0f + erff(z * 0.70710678118654752f));
-  const float pdf = 0.39894228040143268f * __expf(-0.5f * z * z);
-  return cdf + z * pdf;
+  const float z2 = z * z;
+  const float t = tanh_hw(0.7978845608f * fmaf(0.044715f * z, z2, z));
+  return 0.5f * (1.0f + t) + 0.5f * z * (1.0f - t * t) * 0.7978845608f * fmaf(0.134145f, z2, 1.0f);
 }
 
 __device__ __forceinline__ unsigned smem_u32(const void *p) {
@@ -183,7 +195,6 @@ cudaError_t gemm(const GemmArgs &g, int members, cudaStream_t s) {
 // for the bias + GELU epilogue.  Every wait is bounded; a timeout sets
 // *status and the tile is skipped.
 constexpr int TCM = 128;            // rows per tile (UMMA M)
-constexpr int kTcThreads = 256;     // 8 warps
 constexpr int kLboA = (TCM / 8) * 128;
 constexpr long long kTcSpin = 1ll << 22;
 
@@ -227,23 +238,108 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
   return false;
 }
 
+__device__ __forceinline__ void tmem_wait() {
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+}
+
+// 32 consecutive accumulator columns of this warp's 32 tensor-memory lanes.
+__device__ __forceinline__ void tmem_ld32(uint32_t (&v)[32], uint32_t taddr) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+      "%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+        "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+        "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]),
+        "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]),
+        "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+      : "r"(taddr));
+}
+
+// Bias (+ GELU) of 32 accumulator columns [c0, c0+32) of one row; all
+// columns are real (N even multiple of 32 means no padding here).
 template <int EPI>
-__global__ void __launch_bounds__(kTcThreads, 1) tc_layer_kernel(const TcArgs g) {
+__device__ __forceinline__ void epilogue32(const TcArgs &g, const uint32_t (&v)[32], int z, int row,
+                                           int c0, const float *bias) {
+  if (EPI == kTcBiasGelu) {
+    float *zrow = g.Z ? g.Z + z * g.strideZ + (long long)row * g.ldz + c0 : nullptr;
+    uint4 *hrow = reinterpret_cast<uint4 *>(g.H + z * g.strideH + (long long)row * g.ldh + c0);
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      float f[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) f[i] = __uint_as_float(v[b * 8 + i]) + bias[c0 + b * 8 + i];
+      if (zrow) {
+        reinterpret_cast<float4 *>(zrow)[2 * b] = make_float4(f[0], f[1], f[2], f[3]);
+        reinterpret_cast<float4 *>(zrow)[2 * b + 1] = make_float4(f[4], f[5], f[6], f[7]);
+      }
+      __align__(16) __nv_bfloat162 h[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) h[i] = __floats2bfloat162_rn(gelu(f[2 * i]), gelu(f[2 * i + 1]));
+      hrow[b] = *reinterpret_cast<const uint4 *>(h);
+    }
+  } else {
+    float *y = g.Z + z * g.strideZ + (long long)row * g.ldz;
+#pragma unroll
+    for (int i = 0; i < 32; ++i)
+      if (c0 + i < g.n_valid) y[c0 + i] = __uint_as_float(v[i]) + bias[c0 + i];
+  }
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                   bar)
+               : "memory");
+}
+
+// Roles (12 warps): warps 0-2 stream A in K chunks of up to 64 (cp.async,
+// then a proxy fence and an arrive on a_full[chunk]); warp 3, lane 0,
+// issues the MMAs of a tile chunk by chunk into one of two tensor-memory
+// accumulators, releasing each chunk (a_empty) and then the accumulator
+// (acc_full) with tcgen05.commit; warps 4-11 drain an accumulator (bias,
+// GELU, stores) while the next tile's MMAs run, and hand it back
+// (acc_empty).  Every wait is bounded: a timeout sets *status and ends the
+// waiting role; the others then run out of their own waits.
+constexpr int kTcWarps = 12;
+constexpr int kProducers = 96;  // warps 0-2
+
+template <int EPI>
+__global__ void __launch_bounds__(kTcWarps * 32, 1) tc_layer_kernel(const TcArgs g) {
   extern __shared__ __align__(1024) unsigned char smem[];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int z = blockIdx.z;
-  const int m0 = blockIdx.x * TCM;
   const int K = g.K, N = g.N;
+  const int tiles = (g.M + TCM - 1) / TCM;
+  const int KC = K < 64 ? K : 64;  // K per chunk
+  const int nch = K / KC;          // 1..4 chunks
   const uint32_t lboB = (uint32_t)(N / 8) * 128;
   unsigned char *sA = smem;
   unsigned char *sB = smem + (size_t)TCM * K * 2;
-  uint64_t *bar = reinterpret_cast<uint64_t *>(sB + (size_t)K * N * 2);
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 1);
-  const uint32_t sA_u = smem_u32(sA), sB_u = smem_u32(sB), bar_u = smem_u32(bar);
-  const uint32_t ncols = N <= 32 ? 32 : (N <= 64 ? 64 : (N <= 128 ? 128 : 256));
+  float *sBias = reinterpret_cast<float *>(sB + (size_t)K * N * 2);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(sBias + 256);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 12);
+  const uint32_t sA_u = smem_u32(sA), sB_u = smem_u32(sB), bars_u = smem_u32(bars);
+  auto a_full = [&](int c) { return bars_u + 8u * c; };
+  auto a_empty = [&](int c) { return bars_u + 8u * (4 + c); };
+  auto acc_full = [&](int b) { return bars_u + 8u * (8 + b); };
+  auto acc_empty = [&](int b) { return bars_u + 8u * (10 + b); };
+  const uint32_t need = 2u * (uint32_t)N;
+  const uint32_t ncols = need <= 32 ? 32 : need <= 64 ? 64 : need <= 128 ? 128 : need <= 256 ? 256 : 512;
 
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar_u) : "memory");
+    for (int c = 0; c < 4; ++c) {
+      mbar_init(a_full(c), kProducers);
+      mbar_init(a_empty(c), 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(acc_full(b), 1);
+      mbar_init(acc_empty(b), 256);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   if (warp == 0) {
@@ -253,25 +349,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_layer_kernel(const TcArgs g)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
   }
-
-  // Operands into shared memory.  A: 16-byte copies, rows past M zero-filled.
-  const bf16 *A = g.A + z * g.strideA;
-  const int kc8 = K / 8;
-  for (int c = tid; c < TCM * kc8; c += kTcThreads) {
-    const int r_lo = c & 7, rest = c >> 3;
-    const int kc = rest % kc8, r = (rest / kc8) * 8 + r_lo;
-    const uint32_t dst = sA_u + kc * kLboA + (r >> 3) * 128 + r_lo * 16;
-    const int gr = m0 + r;
-    const bf16 *src = A + (long long)(gr < g.M ? gr : 0) * g.lda + kc * 8;
-    const uint32_t bytes = gr < g.M ? 16u : 0u;
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(bytes)
-                 : "memory");
-  }
+  // The layer's weights and bias, once per CTA, by all warps.
   const bf16 *W = g.W + z * g.strideW;
   if (g.n_valid == N) {
-    // W rows of N values: 16-byte copies, k % 8 fastest (one core matrix per 8 lanes)
     const int nc8 = N / 8;
-    for (int c = tid; c < K * nc8; c += kTcThreads) {
+    for (int c = tid; c < K * nc8; c += kTcWarps * 32) {
       const int k_lo = c & 7, rest = c >> 3;
       const int nc = rest % nc8, k = (rest / nc8) * 8 + k_lo;
       const uint32_t dst = sB_u + (k >> 3) * lboB + nc * 128 + k_lo * 16;
@@ -279,99 +361,189 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_layer_kernel(const TcArgs g)
       asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
     }
   } else {
-    // narrow output layer: element copies, columns past n_valid zero
     bf16 *sb = reinterpret_cast<bf16 *>(sB);
-    for (int e = tid; e < K * N; e += kTcThreads) {
+    for (int e = tid; e < K * N; e += kTcWarps * 32) {
       const int k = e / N, n = e % N;
       const bf16 v = n < g.n_valid ? W[(long long)k * g.n_valid + n] : __float2bfloat16(0.0f);
       sb[((k >> 3) * lboB + (n >> 3) * 128 + (k & 7) * 16 + (n & 7) * 2) / 2] = v;
     }
   }
+  const float *bias = g.bias + z * g.strideBias;
+  for (int n = tid; n < N; n += kTcWarps * 32) sBias[n] = n < g.n_valid ? bias[n] : 0.0f;
   asm volatile("cp.async.wait_all;\n" ::: "memory");
   asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   const uint32_t tmem = *tslot;
+  const bf16 *A = g.A + z * g.strideA;
 
-  if (tid == 0) {
-    const uint32_t idesc = (1u << 4)                     // D: FP32
-                           | (1u << 7) | (1u << 10)      // A, B: BF16
-                           | (0u << 15) | (1u << 16)     // A K-major, B MN-major
-                           | ((uint32_t)(N >> 3) << 17)  // N
-                           | ((uint32_t)(TCM >> 4) << 24);  // M
-    for (int j = 0; j < K / 16; ++j) {
-      const uint64_t ad = umma_desc(sA_u + 2 * j * kLboA, kLboA, 128);
-      const uint64_t bd = umma_desc(sB_u + 2 * j * lboB, lboB, 128);
-      const uint32_t acc = j > 0 ? 1u : 0u;
-      asm volatile(
-          "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-          " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
-          "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
-          : "memory");
-    }
-    asm volatile(
-        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
-            bar_u)
-        : "memory");
-  }
-  bool ok = mbar_wait(bar_u, 0);
-  if (!ok) {
-    atomicOr(g.status, 1u);
-    mbar_wait(bar_u, 0);  // a second bounded chance for the MMAs before the memory is freed
-  }
-  ok = __syncthreads_and(ok) != 0;  // the epilogue's tcgen05.ld needs whole warps
-  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-
-  if (ok) {
-    const int q = warp & 3, half = warp >> 2;
-    const int row = m0 + q * 32 + lane;
-    const int c_begin = half * (N / 2), c_end = c_begin + N / 2;
-    const float *bias = g.bias + z * g.strideBias;
-    for (int c0 = c_begin; c0 < c_end; c0 += 8) {
-      uint32_t v[8];
-      const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0;
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
-          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
-            "=r"(v[7])
-          : "r"(taddr));
-      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-      if (row >= g.M) continue;
-      float f[8];
-#pragma unroll
-      for (int i = 0; i < 8; ++i) f[i] = __uint_as_float(v[i]) + (c0 + i < g.n_valid ? bias[c0 + i] : 0.0f);
-      if (EPI == kTcBiasGelu) {
-        if (g.Z) {
-          float4 *zp = reinterpret_cast<float4 *>(g.Z + z * g.strideZ + (long long)row * g.ldz + c0);
-          zp[0] = make_float4(f[0], f[1], f[2], f[3]);
-          zp[1] = make_float4(f[4], f[5], f[6], f[7]);
+  if (warp < 3) {
+    // ---- producers: A tiles chunk by chunk with one chunk of look-ahead:
+    // chunk c is signalled (a_full) once chunk c+1 is issued and c's copies
+    // have landed; before waiting for the MMA to release a chunk, the
+    // pending one is signalled first if it is the one the MMA needs.
+    const int per_chunk = TCM * KC / 8;  // 16-byte copies per chunk
+    int pend_c = -1;
+    auto signal_pending = [&](bool all) {
+      if (all)
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+      else
+        asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      mbar_arrive(a_full(pend_c));
+      pend_c = -1;
+    };
+    bool alive = true;
+    int t = 0;
+    for (int tile = blockIdx.x; tile < tiles && alive; tile += gridDim.x, ++t) {
+      const int m0 = tile * TCM;
+      for (int c = 0; c < nch; ++c) {
+        if (t > 0) {
+          if (pend_c == c) signal_pending(true);  // only with one chunk per tile
+          if (!mbar_wait(a_empty(c), (uint32_t)((t - 1) & 1))) {
+            atomicOr(g.status, 1u);
+            alive = false;
+            break;
+          }
         }
-        __align__(16) bf16 h[8];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) h[i] = __float2bfloat16(gelu(f[i]));
-        *reinterpret_cast<uint4 *>(g.H + z * g.strideH + (long long)row * g.ldh + c0) =
-            *reinterpret_cast<const uint4 *>(h);
-      } else {
-        float *y = g.Z + z * g.strideZ + (long long)row * g.ldz;
-#pragma unroll
-        for (int i = 0; i < 8; ++i)
-          if (c0 + i < g.n_valid) y[c0 + i] = f[i];
+        for (int e = tid; e < per_chunk; e += kProducers) {
+          const int r_lo = e & 7, rest = e >> 3;
+          const int kc = c * (KC / 8) + rest % (KC / 8), r = (rest / (KC / 8)) * 8 + r_lo;
+          const uint32_t dst = sA_u + kc * kLboA + (r >> 3) * 128 + r_lo * 16;
+          const int gr = m0 + r;
+          const bf16 *src = A + (long long)(gr < g.M ? gr : 0) * g.lda + kc * 8;
+          const uint32_t bytes = gr < g.M ? 16u : 0u;
+          asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src),
+                       "r"(bytes)
+                       : "memory");
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+        if (pend_c >= 0) signal_pending(false);
+        pend_c = c;
       }
     }
+    if (pend_c >= 0) signal_pending(true);
+  } else if (warp == 3) {
+    // ---- MMA issuer
+    if (lane == 0) {
+      const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (0u << 15) | (1u << 16) |
+                             ((uint32_t)(N >> 3) << 17) | ((uint32_t)(TCM >> 4) << 24);
+      int t = 0;
+      for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++t) {
+        const int b = t & 1, u = t >> 1;
+        if (u > 0 && !mbar_wait(acc_empty(b), (uint32_t)((u - 1) & 1))) {
+          atomicOr(g.status, 1u);
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        const uint32_t d = tmem + (uint32_t)(b * N);
+        bool ok = true;
+        for (int c = 0; c < nch && ok; ++c) {
+          if (!mbar_wait(a_full(c), (uint32_t)(t & 1))) {
+            atomicOr(g.status, 1u);
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+          for (int j = 0; j < KC / 16; ++j) {
+            const int ks = c * (KC / 16) + j;  // K step of 16
+            const uint64_t ad = umma_desc(sA_u + 2 * ks * kLboA, kLboA, 128);
+            const uint64_t bd = umma_desc(sB_u + 2 * ks * lboB, lboB, 128);
+            const uint32_t acc = ks > 0 ? 1u : 0u;
+            asm volatile(
+                "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d),
+                "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+                : "memory");
+          }
+          umma_commit(a_empty(c));
+        }
+        if (!ok) break;
+        umma_commit(acc_full(b));
+      }
+    }
+    __syncwarp();
+  } else {
+    // ---- epilogue: warp w drains TMEM lanes 32*(w%4).. , column half (w-4)/4
+    const int q = warp & 3, half = (warp - 4) >> 2;
+    const int c_begin = half * (N / 2);
+    int t = 0;
+    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++t) {
+      const int b = t & 1, u = t >> 1;
+      // whole warps or none: tcgen05.ld is warp-collective
+      if (!__all_sync(0xffffffffu, mbar_wait(acc_full(b), (uint32_t)(u & 1)))) {
+        atomicOr(g.status, 1u);
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+      const int row = tile * TCM + q * 32 + lane;
+      const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * N);
+      if ((N / 2) % 32 == 0) {
+        const int chunks = (N / 2) / 32;
+        uint32_t va[32], vb[32];
+        tmem_ld32(va, tbase + c_begin);
+        tmem_wait();
+        for (int c = 0; c < chunks; c += 2) {
+          if (c + 1 < chunks) tmem_ld32(vb, tbase + c_begin + (c + 1) * 32);
+          if (row < g.M) epilogue32<EPI>(g, va, z, row, c_begin + c * 32, sBias);
+          tmem_wait();
+          if (c + 1 < chunks) {
+            if (c + 2 < chunks) tmem_ld32(va, tbase + c_begin + (c + 2) * 32);
+            if (row < g.M) epilogue32<EPI>(g, vb, z, row, c_begin + (c + 1) * 32, sBias);
+            tmem_wait();
+          }
+        }
+      } else {
+        for (int c0 = c_begin; c0 < c_begin + N / 2; c0 += 8) {
+          uint32_t v[8];
+          asm volatile(
+              "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+              : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+                "=r"(v[6]), "=r"(v[7])
+              : "r"(tbase + (uint32_t)c0));
+          tmem_wait();
+          if (row >= g.M) continue;
+          float f[8];
+#pragma unroll
+          for (int i = 0; i < 8; ++i) f[i] = __uint_as_float(v[i]) + sBias[c0 + i];
+          if (EPI == kTcBiasGelu) {
+            if (g.Z) {
+              float4 *zp = reinterpret_cast<float4 *>(g.Z + z * g.strideZ + (long long)row * g.ldz + c0);
+              zp[0] = make_float4(f[0], f[1], f[2], f[3]);
+              zp[1] = make_float4(f[4], f[5], f[6], f[7]);
+            }
+            __align__(16) bf16 h[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) h[i] = __float2bfloat16(gelu(f[i]));
+            *reinterpret_cast<uint4 *>(g.H + z * g.strideH + (long long)row * g.ldh + c0) =
+                *reinterpret_cast<const uint4 *>(h);
+          } else {
+            float *y = g.Z + z * g.strideZ + (long long)row * g.ldz;
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+              if (c0 + i < g.n_valid) y[c0 + i] = f[i];
+          }
+        }
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+      mbar_arrive(acc_empty(b));
+    }
   }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   __syncthreads();
-  if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem),
-                 "r"(ncols)
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(ncols)
                  : "memory");
+  }
 }
 
 size_t tc_smem_bytes(int K, int N) {
   // operands + mbarrier + TMEM slot; at least 120 KB so that one CTA runs
   // per SM and its tensor-memory allocation never waits for another's
-  const size_t need = (size_t)TCM * K * 2 + (size_t)K * N * 2 + 16;
+  const size_t need = (size_t)TCM * K * 2 + (size_t)K * N * 2 + 256 * 4 + 12 * 8 + 16;
   return std::max<size_t>(need, 120 * 1024);
 }
 
@@ -391,8 +563,17 @@ cudaError_t tc_layer(const TcArgs &g, int members, cudaStream_t s) {
     if (e != cudaSuccess) return e;
     configured[dev] = true;
   }
-  dim3 grid((g.M + TCM - 1) / TCM, 1, members);
-  tc_layer_kernel<EPI><<<grid, kTcThreads, smem, s>>>(g);
+  static int sms[64] = {};
+  if (!sms[dev]) {
+    e = cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+  }
+  // persistent: one CTA per SM shared out among the members, each CTA
+  // walking its member's 128-row tiles with the weights resident
+  const int tiles = (g.M + TCM - 1) / TCM;
+  const int per_member = std::max(1, sms[dev] / std::max(1, members));
+  dim3 grid(std::min(tiles, per_member), 1, members);
+  tc_layer_kernel<EPI><<<grid, kTcWarps * 32, smem, s>>>(g);
   return cudaGetLastError();
 }
 

@@ -21,13 +21,17 @@ def bf(a):
     return torch.as_tensor(a, dtype=torch.float64).to(torch.bfloat16).to(torch.float64)
 
 
+C_GELU = np.sqrt(2.0 / np.pi)
+
+
 def gelu(z):
-    return 0.5 * z * (1.0 + torch.erf(z / np.sqrt(2.0)))
+    """GELU, tanh form (the kernels' activation)."""
+    return 0.5 * z * (1.0 + torch.tanh(C_GELU * (z + 0.044715 * z ** 3)))
 
 
 def gelu_grad(z):
-    cdf = 0.5 * (1.0 + torch.erf(z / np.sqrt(2.0)))
-    return cdf + z * torch.exp(-0.5 * z * z) / np.sqrt(2 * np.pi)
+    t = torch.tanh(C_GELU * (z + 0.044715 * z ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * z * (1.0 - t * t) * C_GELU * (1.0 + 3 * 0.044715 * z * z)
 
 
 def cpu_reference(params, shapes, X, T, xm, xs, tm, ts):
