@@ -213,6 +213,7 @@ struct TcArgs {
   bf16 *H;                  // kTcBiasGelu: activations
   long long ldh, strideH;
   unsigned *status;
+  int slots;                // A ring slots (chunks of up to 64 K columns), 2..16
 };
 
 __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
@@ -297,8 +298,9 @@ __device__ __forceinline__ void umma_commit(uint32_t bar) {
                : "memory");
 }
 
-// Roles (12 warps): warps 0-2 stream A in K chunks of up to 64 (cp.async,
-// then a proxy fence and an arrive on a_full[chunk]); warp 3, lane 0,
+// Roles (12 warps): warps 0-2 stream A in K chunks of up to 64 into a ring
+// of shared-memory slots (cp.async, completion arriving on a_full[slot]);
+// warp 3, lane 0,
 // issues the MMAs of a tile chunk by chunk into one of two tensor-memory
 // accumulators, releasing each chunk (a_empty) and then the accumulator
 // (acc_full) with tcgen05.commit; warps 4-11 drain an accumulator (bias,
@@ -316,23 +318,25 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1) tc_layer_kernel(const TcArgs
   const int K = g.K, N = g.N;
   const int tiles = (g.M + TCM - 1) / TCM;
   const int KC = K < 64 ? K : 64;  // K per chunk
-  const int nch = K / KC;          // 1..4 chunks
+  const int nch = K / KC;          // 1..4 chunks per tile
+  const int nslots = g.slots;      // A ring: chunk i of the CTA's sequence uses slot i % nslots
+  const uint32_t slot_bytes = (uint32_t)(KC / 8) * kLboA;
   const uint32_t lboB = (uint32_t)(N / 8) * 128;
-  unsigned char *sA = smem;
-  unsigned char *sB = smem + (size_t)TCM * K * 2;
-  float *sBias = reinterpret_cast<float *>(sB + (size_t)K * N * 2);
+  unsigned char *sB = smem;
+  unsigned char *sA = smem + (size_t)K * N * 2;
+  float *sBias = reinterpret_cast<float *>(sA + (size_t)nslots * slot_bytes);
   uint64_t *bars = reinterpret_cast<uint64_t *>(sBias + 256);
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 12);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 36);
   const uint32_t sA_u = smem_u32(sA), sB_u = smem_u32(sB), bars_u = smem_u32(bars);
-  auto a_full = [&](int c) { return bars_u + 8u * c; };
-  auto a_empty = [&](int c) { return bars_u + 8u * (4 + c); };
-  auto acc_full = [&](int b) { return bars_u + 8u * (8 + b); };
-  auto acc_empty = [&](int b) { return bars_u + 8u * (10 + b); };
+  auto a_full = [&](int s) { return bars_u + 8u * s; };
+  auto a_empty = [&](int s) { return bars_u + 8u * (16 + s); };
+  auto acc_full = [&](int b) { return bars_u + 8u * (32 + b); };
+  auto acc_empty = [&](int b) { return bars_u + 8u * (34 + b); };
   const uint32_t need = 2u * (uint32_t)N;
   const uint32_t ncols = need <= 32 ? 32 : need <= 64 ? 64 : need <= 128 ? 128 : need <= 256 ? 256 : 512;
 
   if (tid == 0) {
-    for (int c = 0; c < 4; ++c) {
+    for (int c = 0; c < nslots; ++c) {
       mbar_init(a_full(c), kProducers);
       mbar_init(a_empty(c), 1);
     }
@@ -379,51 +383,41 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1) tc_layer_kernel(const TcArgs
   const bf16 *A = g.A + z * g.strideA;
 
   if (warp < 3) {
-    // ---- producers: A tiles chunk by chunk with one chunk of look-ahead:
-    // chunk c is signalled (a_full) once chunk c+1 is issued and c's copies
-    // have landed; before waiting for the MMA to release a chunk, the
-    // pending one is signalled first if it is the one the MMA needs.
+    // ---- producers: A chunks into the ring.  Each thread's copies of a
+    // chunk arrive on a_full[slot] by themselves when they land
+    // (cp.async.mbarrier.arrive.noinc; the barrier expects all 96 producer
+    // threads), so the producers never wait for their own copies and run as
+    // far ahead as the ring allows: a slot is refilled once the MMAs of the
+    // chunk that used it last have completed (a_empty).
     const int per_chunk = TCM * KC / 8;  // 16-byte copies per chunk
-    int pend_c = -1;
-    auto signal_pending = [&](bool all) {
-      if (all)
-        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-      else
-        asm volatile("cp.async.wait_group 1;\n" ::: "memory");
-      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-      mbar_arrive(a_full(pend_c));
-      pend_c = -1;
-    };
-    bool alive = true;
-    int t = 0;
-    for (int tile = blockIdx.x; tile < tiles && alive; tile += gridDim.x, ++t) {
+    int gi = 0;                          // chunk sequence number
+    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
       const int m0 = tile * TCM;
-      for (int c = 0; c < nch; ++c) {
-        if (t > 0) {
-          if (pend_c == c) signal_pending(true);  // only with one chunk per tile
-          if (!mbar_wait(a_empty(c), (uint32_t)((t - 1) & 1))) {
-            atomicOr(g.status, 1u);
-            alive = false;
-            break;
-          }
+      bool alive = true;
+      for (int c = 0; c < nch; ++c, ++gi) {
+        const int slot = gi % nslots, use = gi / nslots;
+        if (use > 0 && !mbar_wait(a_empty(slot), (uint32_t)((use - 1) & 1))) {
+          atomicOr(g.status, 1u);
+          alive = false;
+          break;
         }
+        const uint32_t base = sA_u + (uint32_t)slot * slot_bytes;
         for (int e = tid; e < per_chunk; e += kProducers) {
           const int r_lo = e & 7, rest = e >> 3;
-          const int kc = c * (KC / 8) + rest % (KC / 8), r = (rest / (KC / 8)) * 8 + r_lo;
-          const uint32_t dst = sA_u + kc * kLboA + (r >> 3) * 128 + r_lo * 16;
+          const int kl = rest % (KC / 8), r = (rest / (KC / 8)) * 8 + r_lo;
+          const uint32_t dst = base + kl * kLboA + (r >> 3) * 128 + r_lo * 16;
           const int gr = m0 + r;
-          const bf16 *src = A + (long long)(gr < g.M ? gr : 0) * g.lda + kc * 8;
+          const bf16 *src = A + (long long)(gr < g.M ? gr : 0) * g.lda + (c * (KC / 8) + kl) * 8;
           const uint32_t bytes = gr < g.M ? 16u : 0u;
           asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src),
                        "r"(bytes)
                        : "memory");
         }
-        asm volatile("cp.async.commit_group;\n" ::: "memory");
-        if (pend_c >= 0) signal_pending(false);
-        pend_c = c;
+        asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(a_full(slot))
+                     : "memory");
       }
+      if (!alive) break;
     }
-    if (pend_c >= 0) signal_pending(true);
   } else if (warp == 3) {
     // ---- MMA issuer
     if (lane == 0) {
@@ -440,15 +434,17 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1) tc_layer_kernel(const TcArgs
         const uint32_t d = tmem + (uint32_t)(b * N);
         bool ok = true;
         for (int c = 0; c < nch && ok; ++c) {
-          if (!mbar_wait(a_full(c), (uint32_t)(t & 1))) {
+          const int gi = t * nch + c, slot = gi % nslots, use = gi / nslots;
+          if (!mbar_wait(a_full(slot), (uint32_t)(use & 1))) {
             atomicOr(g.status, 1u);
             ok = false;
             break;
           }
           asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+          const uint32_t base = sA_u + (uint32_t)slot * slot_bytes;
           for (int j = 0; j < KC / 16; ++j) {
-            const int ks = c * (KC / 16) + j;  // K step of 16
-            const uint64_t ad = umma_desc(sA_u + 2 * ks * kLboA, kLboA, 128);
+            const int ks = c * (KC / 16) + j;  // K step of 16 within the tile
+            const uint64_t ad = umma_desc(base + 2 * j * kLboA, kLboA, 128);
             const uint64_t bd = umma_desc(sB_u + 2 * ks * lboB, lboB, 128);
             const uint32_t acc = ks > 0 ? 1u : 0u;
             asm volatile(
@@ -457,7 +453,7 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1) tc_layer_kernel(const TcArgs
                 "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
                 : "memory");
           }
-          umma_commit(a_empty(c));
+          umma_commit(a_empty(slot));
         }
         if (!ok) break;
         umma_commit(acc_full(b));
@@ -540,10 +536,21 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1) tc_layer_kernel(const TcArgs
   }
 }
 
-size_t tc_smem_bytes(int K, int N) {
-  // operands + mbarrier + TMEM slot; at least 120 KB so that one CTA runs
-  // per SM and its tensor-memory allocation never waits for another's
-  const size_t need = (size_t)TCM * K * 2 + (size_t)K * N * 2 + 256 * 4 + 12 * 8 + 16;
+constexpr size_t kTcSmemMax = 227 * 1024;  // opt-in shared memory per block
+constexpr size_t kTcSmemFixed = 256 * 4 + 36 * 8 + 16;  // bias, barriers, TMEM slot
+
+size_t tc_slot_bytes(int K) { return (size_t)(K < 64 ? K : 64) / 8 * kLboA; }
+
+// A ring slots: as many as fit beside the weights (at most 16).
+int tc_slots(int K, int N) {
+  const size_t room = kTcSmemMax - (size_t)K * N * 2 - kTcSmemFixed;
+  return (int)std::min<size_t>(16, room / tc_slot_bytes(K));
+}
+
+size_t tc_smem_bytes(int K, int N, int slots) {
+  // at least 120 KB so that one CTA runs per SM and its tensor-memory
+  // allocation never waits for another's
+  const size_t need = (size_t)K * N * 2 + (size_t)slots * tc_slot_bytes(K) + kTcSmemFixed;
   return std::max<size_t>(need, 120 * 1024);
 }
 
@@ -551,7 +558,10 @@ template <int EPI>
 cudaError_t tc_layer(const TcArgs &g, int members, cudaStream_t s) {
   if (g.N % 16 || g.N < 16 || g.N > 256 || g.K % 16 || g.K < 16 || g.K > 256 || g.n_valid > g.N)
     return cudaErrorInvalidValue;
-  const size_t smem = tc_smem_bytes(g.K, g.N);
+  TcArgs a = g;
+  a.slots = tc_slots(g.K, g.N);
+  if (a.slots < 2) return cudaErrorInvalidValue;
+  const size_t smem = tc_smem_bytes(g.K, g.N, a.slots);
   static bool configured[64] = {};  // per device: the attribute is per context
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -559,7 +569,7 @@ cudaError_t tc_layer(const TcArgs &g, int members, cudaStream_t s) {
   if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
   if (!configured[dev]) {
     e = cudaFuncSetAttribute(tc_layer_kernel<EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             200 * 1024);
+                             (int)kTcSmemMax);
     if (e != cudaSuccess) return e;
     configured[dev] = true;
   }
@@ -573,7 +583,7 @@ cudaError_t tc_layer(const TcArgs &g, int members, cudaStream_t s) {
   const int tiles = (g.M + TCM - 1) / TCM;
   const int per_member = std::max(1, sms[dev] / std::max(1, members));
   dim3 grid(std::min(tiles, per_member), 1, members);
-  tc_layer_kernel<EPI><<<grid, kTcWarps * 32, smem, s>>>(g);
+  tc_layer_kernel<EPI><<<grid, kTcWarps * 32, smem, s>>>(a);
   return cudaGetLastError();
 }
 
