@@ -9,6 +9,11 @@
 //   -T <slots>     RNG subsequences ("photon slots"); default = the
 //                  reference's thread count on the selected GPU
 //   -grid nr nz dr dz   absorbance grid (default 1000 500 0.01 0.01)
+//   -CK <file>     checkpointed first pass: launches of a slice of the slots,
+//                  the file brought up to date after each, a run resumes
+//                  from it when it exists (<file>.<i> for simulation i > 0)
+//   -batch         every simulation of the file in one batched launch
+//                  (first pass only: output.txt and summary.json)
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -38,6 +43,8 @@ void show_usage(const std::string &name) {
             << "\t-S,\t\t Seed of the random number generator (default: time(NULL))\n"
             << "\t-T,\t\t Number of photon slots / RNG subsequences (default: reference layout)\n"
             << "\t-grid,\t\t Absorbance grid: nr nz dr dz (default: 1000 500 0.01 0.01)\n"
+            << "\t-CK,\t\t Checkpoint file of the first pass, following by a path (resumes if present)\n"
+            << "\t-batch,\t\t Run all simulations in one batched launch (no -R)\n"
             << std::endl;
 }
 
@@ -79,6 +86,8 @@ int main(int argc, char *argv[]) {
   unsigned long long slots = 0;
   unsigned grid_nr = 0, grid_nz = 0;
   float grid_dr = 0, grid_dz = 0;
+  std::string checkpoint;
+  bool do_batch = false;
 
   for (int i = 1; i < argc; i++) {
     const std::string a(argv[i]);
@@ -126,6 +135,10 @@ int main(int argc, char *argv[]) {
       grid_dr = std::strtof(argv[i + 3], nullptr);
       grid_dz = std::strtof(argv[i + 4], nullptr);
       i += 4;
+    } else if (a == "-CK" && i + 1 < argc) {
+      checkpoint = argv[++i];
+    } else if (a == "-batch") {
+      do_batch = true;
     }
   }
 
@@ -148,6 +161,10 @@ int main(int argc, char *argv[]) {
   }
   if (do_B && !(do_P || do_A)) {
     std::cout << "-B option only work with -P or -A option!\n";
+    return 0;
+  }
+  if (do_batch && (do_replay || !checkpoint.empty())) {
+    std::cout << "-batch option does not work with -R or -CK option!\n";
     return 0;
   }
 
@@ -181,6 +198,48 @@ int main(int argc, char *argv[]) {
   if (do_B) flags |= MCML_OUT_BINARY;
 
   const auto t_all = std::chrono::steady_clock::now();
+  if (do_batch) {
+    mcml_batch_opts bo{};
+    bo.seed = seed;
+    bo.device = gpu;
+    mcml_batch *b = nullptr;
+    int rc = mcml_batch_create(sims.data(), n_sims, &bo, &b);
+    if (rc == MCML_OK) rc = mcml_batch_autotune(b, 1.0 / 64, nullptr);
+    std::vector<mcml_result> res(n_sims);
+    const auto t0 = std::chrono::steady_clock::now();
+    if (rc == MCML_OK) rc = mcml_batch_run(b, res.data());
+    const auto t1 = std::chrono::steady_clock::now();
+    if (rc != MCML_OK) {
+      std::printf("Error: %s (%s)\n", mcml_strerror(rc), mcml_last_error());
+      if (b) mcml_batch_destroy(b);
+      return 1;
+    }
+    mcml_batch_destroy(b);
+    mcml_device_info info{};
+    mcml_get_device_info(gpu, &info);
+    const double sim_s = std::chrono::duration<double>(t1 - t0).count();
+    for (int i = 0; i < n_sims; i++) {
+      std::vector<uint64_t> det(res[i].num_sds);
+      for (unsigned d = 0; d < res[i].num_sds; d++) det[d] = res[i].detected[d];
+      mcml_host_data hd{};
+      hd.photons = sims[i].number_photons;
+      hd.detected = det.data();
+      hd.weight_sum = res[i].weight_sum;
+      hd.gpu_name = info.name;
+      rc = mcml_write_host_outputs(&sims[i], &hd, "", argv[3], 0, sim_s / n_sims, 0.0);
+      if (rc != MCML_OK) {
+        std::printf("Error: %s (%s)\n", mcml_strerror(rc), mcml_last_error());
+        return 1;
+      }
+      std::printf("simulation %d:", i);
+      for (unsigned d = 0; d < res[i].num_sds; d++)
+        std::printf(" SDS %u %.6e +- %.2e;", d + 1, res[i].reflectance[d], res[i].std_error[d]);
+      std::printf("\n");
+    }
+    std::printf("Simulation time: %.2f sec\n",
+                std::chrono::duration<double>(std::chrono::steady_clock::now() - t_all).count());
+    return 0;
+  }
   for (int i = 0; i < n_sims; i++) {
     std::printf("simulating %d\n", i);
     mcml_opts opts{};
@@ -199,7 +258,14 @@ int main(int argc, char *argv[]) {
     }
     const auto t0 = std::chrono::steady_clock::now();
     mcml_result res{};
-    rc = mcml_run(ctx, &res);
+    if (checkpoint.empty()) {
+      rc = mcml_run(ctx, &res);
+    } else {
+      const std::string path = i == 0 ? checkpoint : checkpoint + "." + std::to_string(i);
+      mcml_checkpoint_opts ck{};
+      ck.path = path.c_str();
+      rc = mcml_run_checkpointed(ctx, &ck, &res);
+    }
     const auto t1 = std::chrono::steady_clock::now();
     if (rc != MCML_OK) {
       std::printf("Error: %s (%s)\n", mcml_strerror(rc), mcml_last_error());

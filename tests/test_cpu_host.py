@@ -137,7 +137,10 @@ def test_cli_usage_and_flag_rules():
                        (["-A"], "-A option only work with -R option!"),
                        (["-AP"], "-AP option only work with -R option!"),
                        (["-R", "-B"], None),
-                       (["-B"], "-B option only work with -P or -A option!")]:
+                       (["-B"], "-B option only work with -P or -A option!"),
+                       (["-batch", "-R"], "-batch option does not work with -R or -CK option!"),
+                       (["-batch", "-CK", "x.ckpt"],
+                        "-batch option does not work with -R or -CK option!")]:
         r = run_cli(str(sj), str(it), "out.txt", *flags, cwd=tempfile.gettempdir())
         if msg:
             assert r.returncode == 0 and msg in r.stdout, (flags, r.stdout)
