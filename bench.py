@@ -248,9 +248,12 @@ def batch_arm(args) -> int:
         for _ in range(max(args.warmup, 1)):
             b.run()
         times = []
+        sampler = ClockSampler(0)
+        sampler.start()
         for _ in range(args.steps):
             res = b.run()
             times.append(res[0].walk_ms)
+        clocks = sampler.stop()
     ms = sum(times) / len(times)
     steps = sum(int(r.steps) for r in res)
     # the same sets one at a time through mcml_run (sample of 32 sets)
@@ -274,10 +277,98 @@ def batch_arm(args) -> int:
                              "photons_per_slot": tuning.photons_per_slot},
                    "tune_s": round(tune_s, 2), "cuda_graph": True},
         "steps_per_s": steps / (ms / 1e3),
+        "roofline": issue_roofline(steps / (ms / 1e3), clocks, "batch_walk_kernel"),
+        "clocks": clocks,
         "sequential_same_library": {"value": seq_photons / (seq_ms / 1e3), "sets": len(sample)},
         "median_rel_se_sds2": float(np.median(rel)) if rel else None,
     }), flush=True)
     return 0
+
+
+def issue_roofline(steps_per_s: float, clocks: dict, kernel: str) -> dict:
+    """Walk steps/s against the issue bound of the hand-counted step (see
+    OPS_LANE / OPS_MUFU) at the median SM clock sampled while it ran."""
+    f_sm = clocks.get("sm_mhz") or 1965.0
+    peak = f_sm * 1e6 * SM_COUNT * steps_per_clock_per_sm()
+    return {"bound": "issue", "achieved": steps_per_s / 1e9, "peak": peak / 1e9,
+            "unit": "Gstep/s", "frac": steps_per_s / peak, "kernel": kernel}
+
+
+def wmc_arm(args) -> int:
+    """White-MC relabelling throughput: the replayed photons of one SDS of
+    the ring geometry (tests/golden/configs/surrogate, 2e7 photons) under
+    4096 (mua', mus') combinations; one term = one (photon, combo) pair:
+    K = 2L+2 FMAs, one exp2, one add.  Timed with CUDA events on the
+    launching stream after warm-up."""
+    import torch
+    import mcml_gpu_b200 as m
+    import mcml_gpu_b200.wmc as wmc
+    cfg = ROOT / "tests" / "golden" / "configs" / "surrogate"
+    sim = m.parse_config(cfg / "sim_set.json", cfg / "input.txt")[0]
+    sim.number_photons = int(args.photons) if args.photons else 20_000_000
+    L = int(sim.num_layers)
+    with m.Simulation(sim, seed=args.seed) as run:
+        run.run()
+        run.replay()
+        rows, inter = run.rows(1)
+    rng = np.random.default_rng(3)
+    C = 4096
+    mua0 = np.array([sim.mua[l] for l in range(L)])
+    mus0 = np.array([sim.mus[l] for l in range(L)])
+    combos = np.hstack([rng.uniform(0.05, 0.5, (C, L)),
+                        mus0[None, :] * rng.uniform(0.95, 1.05, (C, L))]).astype(np.float32)
+    combos_t = torch.from_numpy(combos).cuda()
+    prep = wmc.Prepared(rows, inter)
+    for _ in range(max(args.warmup, 1)):
+        prep.rescale(mua0, mus0, combos_t, int(sim.number_photons))
+    torch.cuda.synchronize()
+    sampler = ClockSampler(0)
+    sampler.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(args.steps):
+        out = prep.rescale(mua0, mus0, combos_t, int(sim.number_photons))
+    ev1.record()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    D = rows.shape[0]
+    terms = D * C / (ms / 1e3)
+    K = 2 * L + 2
+    ops = K + 1 + 1 + 2 + K / 4  # FMAs, exp2 (MUFU), add, exp2 range handling, shared loads
+    f_sm = clocks.get("sm_mhz") or 1965.0
+    peak = f_sm * 1e6 * SM_COUNT * min(128.0 / ops, 16.0)
+    print(json.dumps({
+        "metric": "White-MC terms/s", "impl": "mcml-wmc", "value": terms, "unit": "terms/s",
+        "ms_per_step": ms, "steps": args.steps, "warmup": args.warmup,
+        "config": {"workload": f"WMC rescale, ring geometry, {sim.number_photons:.3g} photons, "
+                               f"SDS 1: {D} replayed photons x {C} combos, L={L}",
+                   "includes": "coefficient and packing kernels of each call (inputs resident)"},
+        "roofline": {"bound": "issue", "achieved": terms / 1e12, "peak": peak / 1e12,
+                     "unit": "Tterm/s", "frac": terms / peak,
+                     "model": f"{ops:.0f} thread-ops per term, 128 per clk per SM"},
+        "clocks": clocks}), flush=True)
+    return 0
+
+
+def measured_peak(key: str, fallback: float) -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        return float(json.loads(p.read_text())[key]), "measured"
+    except Exception:
+        return fallback, "fallback"
+
+
+def mlp_roofline(queries: int, seconds: float) -> dict:
+    """Tensor-core roofline of ensemble inference: algorithmic FLOPs of the
+    25 -> 256x4 -> 3 network x 4 members per query (2 x MACs, real widths),
+    over the whole predict call (gather, layers, ensemble reduction)."""
+    macs = 25 * 256 + 3 * 256 * 256 + 256 * 3
+    flops = 2.0 * macs * 4 * queries
+    peak, kind = measured_peak("bf16_tflops", 1590.0)
+    achieved = flops / seconds / 1e12
+    return {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": achieved / peak, "peak_kind": kind, "flop_per_query": 2.0 * macs * 4}
 
 
 def reference_plain_mc_evals(cfg: Path, sims, photons: int) -> tuple[float | None, str]:
@@ -401,6 +492,7 @@ def surrogate_arm(args) -> int:
         "metric": "SDS-reflectance evals/s", "impl": "mcml-surrogate",
         "value": nq / serve_s, "unit": "evals/s",
         "mlp_only_evals_per_s": nq / mlp_s,
+        "mlp_roofline": mlp_roofline(nq, mlp_s),
         "plain_mc_evals_per_s_at_ref_photons": mc_evals,
         "speedup_vs_plain_mc": (nq / serve_s) / mc_evals,
         "speedup_vs_plain_mc_inside_hull": (nq / mlp_s) / mc_evals,
@@ -582,7 +674,7 @@ def main() -> int:
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mcml",
-                    choices=["mcml", "reference", "reference-gpu", "batch", "surrogate"])
+                    choices=["mcml", "reference", "reference-gpu", "batch", "surrogate", "wmc"])
     ap.add_argument("--photons", type=int, default=0, help="override N (default: 1e8)")
     ap.add_argument("--slots", type=int, default=0)
     ap.add_argument("--block", type=int, default=0)
@@ -610,6 +702,8 @@ def main() -> int:
         return batch_arm(args)
     if args.impl == "surrogate":
         return surrogate_arm(args)
+    if args.impl == "wmc":
+        return wmc_arm(args)
     return mcml_arm(args)
 
 

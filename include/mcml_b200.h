@@ -92,7 +92,7 @@ typedef struct mcml_opts {
                                the reference's thread count on this device
                                (SMs x max threads/SM, io.cpp:522-526) -- its
                                one-photon-per-thread layout, bit-exact when N equals
-                               it -- else about 8 photons per slot.                  */
+                               it -- else about 4 photons per slot.                  */
   int32_t device;           /* CUDA ordinal (reference: -G, main.cu:51-59)          */
   uint32_t grid_nr;         /* absorbance grid; 0 = 1000                            */
   uint32_t grid_nz;         /* 0 = 500                                              */

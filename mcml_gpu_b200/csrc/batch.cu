@@ -564,7 +564,7 @@ int mcml_batch_autotune(mcml_batch *b, double photon_fraction, mcml_batch_tuning
   o.seed = b->seed;
   o.stream = b->stream;
   o.no_graph = 1;
-  const uint32_t pps[] = {8, 32, 128};
+  const uint32_t pps[] = {4, 8, 32};
   double best = 1e300;
   int best_v = b->variant;
   uint32_t best_pps = b->photons_per_slot;

@@ -67,7 +67,7 @@ constexpr uint64_t kDefaultBudget = 1ull << 26;
 // Automatic slot count for N above the reference's thread count: about
 // this many photons per slot keeps the end-of-launch tail (one slot of
 // work) small against each lane's share, at one skipahead per slot.
-constexpr uint64_t kPhotonsPerSlot = 8;
+constexpr uint64_t kPhotonsPerSlot = 4;
 constexpr uint64_t kMaxAutoSlots = 1ull << 26;
 
 }  // namespace

@@ -22,9 +22,11 @@
 // contraction, one exp2 (MUFU) and one add.  The exponents reach hundreds,
 // so the contraction stays in FP32 on the CUDA cores (a bf16/tf32 tensor
 // product would lose the exponent's low bits).  Photon features are staged
-// through shared memory in chunks and each thread carries kPer combos.
+// through shared memory in chunks and each thread carries kPer combos;
+// the photons are split over blockIdx.y and the partial sums added in FP64.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <string>
 
@@ -70,8 +72,13 @@ __global__ void __launch_bounds__(kThreads) wmc_kernel(const float *F, uint64_t 
 #pragma unroll
   for (int r = 0; r < kPer; ++r) total[r] = 0.0;
 
-  for (uint64_t base = 0; base < D; base += kChunk) {
-    const int n = (int)((D - base) < (uint64_t)kChunk ? (D - base) : (uint64_t)kChunk);
+  // this block's share of the photons (blockIdx.y of gridDim.y, whole chunks)
+  const uint64_t chunks = (D + kChunk - 1) / kChunk;
+  const uint64_t per = (chunks + gridDim.y - 1) / gridDim.y;
+  const uint64_t d0 = blockIdx.y * per * kChunk;
+  const uint64_t d1 = d0 + per * kChunk < D ? d0 + per * kChunk : D;
+  for (uint64_t base = d0; base < d1; base += kChunk) {
+    const int n = (int)((d1 - base) < (uint64_t)kChunk ? (d1 - base) : (uint64_t)kChunk);
     __syncthreads();
     for (int idx = threadIdx.x; idx < n * K; idx += kThreads) {
       const int j = idx / K, k = idx % K;
@@ -99,7 +106,7 @@ __global__ void __launch_bounds__(kThreads) wmc_kernel(const float *F, uint64_t 
   }
 #pragma unroll
   for (int r = 0; r < kPer; ++r)
-    if (c0 + r < C) out[c0 + r] = total[r] * inv_scale;
+    if (c0 + r < C && d0 < d1) atomicAdd(&out[c0 + r], total[r] * inv_scale);
 }
 
 // Per-combo coefficient rows a_c (padded to kMaxK).
@@ -123,9 +130,19 @@ __global__ void wmc_coef_kernel(const float *combos, uint64_t C, int L, const fl
 template <int K>
 cudaError_t launch_wmc(const float *F, uint64_t D, const float *coef, uint64_t C,
                        double inv_scale, double *out, cudaStream_t s) {
+  // combos across blockIdx.x, photons split across blockIdx.y so that a
+  // few hundred combos still fill every SM; partial sums meet in FP64 atomics
   const uint64_t per_block = (uint64_t)kThreads * kPer;
-  const unsigned grid = (unsigned)((C + per_block - 1) / per_block);
-  wmc_kernel<K><<<grid, kThreads, 0, s>>>(F, D, coef, C, inv_scale, out);
+  const unsigned gx = (unsigned)((C + per_block - 1) / per_block);
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const uint64_t chunks = (D + kChunk - 1) / kChunk;
+  const uint64_t want = ((uint64_t)4 * sms + gx - 1) / gx;
+  const unsigned gy = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(std::min<uint64_t>(chunks, want), 65535));
+  cudaError_t e = cudaMemsetAsync(out, 0, C * sizeof(double), s);
+  if (e != cudaSuccess) return e;
+  wmc_kernel<K><<<dim3(gx, gy), kThreads, 0, s>>>(F, D, coef, C, inv_scale, out);
   return cudaGetLastError();
 }
 

@@ -13,7 +13,7 @@ import numpy as np
 
 from . import MAX_LAYERS, _check, load_library
 
-__all__ = ["WmcSet", "rescale", "rescale_reference"]
+__all__ = ["WmcSet", "Prepared", "rescale", "rescale_reference"]
 
 
 class WmcSet(C.Structure):
@@ -38,6 +38,47 @@ def _bind(lib):
     lib._wmc_bound = True
 
 
+class Prepared:
+    """Replay rows and interaction counts of one SDS on the device, in the
+    layer-major layout mcml_wmc_rescale reads."""
+
+    def __init__(self, rows: np.ndarray, interactions: np.ndarray, device: int = 0):
+        import torch
+        dev = torch.device("cuda", device)
+        rows = np.asarray(rows, dtype=np.float32)
+        self.L = rows.shape[1] - 2
+        self.D = rows.shape[0]
+        self.device = device
+        self.pl = torch.from_numpy(np.ascontiguousarray(rows[:, 1:self.L + 1].T)).to(dev)
+        self.ni = torch.from_numpy(
+            np.ascontiguousarray(np.asarray(interactions, np.float32).T)).to(dev)
+        self.w = torch.from_numpy(np.ascontiguousarray(rows[:, 0])).to(dev)
+        self._ws = None
+
+    def rescale(self, base_mua, base_mus, combos, photons: int):
+        """combos: (C, 2L) CUDA float32 tensor.  Returns C float64 reflectances
+        (CUDA tensor), enqueued on the current torch stream."""
+        import torch
+        lib = load_library()
+        _bind(lib)
+        dev = torch.device("cuda", self.device)
+        Cn = combos.shape[0]
+        out = torch.empty(Cn, dtype=torch.float64, device=dev)
+        nbytes = int(lib.mcml_wmc_workspace_bytes(self.D, Cn))
+        if self._ws is None or self._ws.numel() < nbytes:
+            self._ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+        s = WmcSet(self.pl.data_ptr(), self.ni.data_ptr(), self.w.data_ptr(), self.D, self.L)
+        bm = (C.c_float * MAX_LAYERS)(*[float(v) for v in base_mua][:self.L])
+        bs = (C.c_float * MAX_LAYERS)(*[float(v) for v in base_mus][:self.L])
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        _check(lib.mcml_wmc_rescale(C.byref(s), bm, bs, C.c_void_p(combos.data_ptr()), Cn,
+                                    float(0xFFFFFFFF) * float(photons), C.c_void_p(out.data_ptr()),
+                                    C.c_void_p(self._ws.data_ptr()), self._ws.numel(),
+                                    C.c_void_p(stream)),
+               "mcml_wmc_rescale")
+        return out
+
+
 def rescale(rows: np.ndarray, interactions: np.ndarray, base_mua, base_mus, combos, photons: int,
             device: int = 0):
     """rows: (D, L+2) float32 replay rows (weight, PL_1..L, steps);
@@ -45,31 +86,11 @@ def rescale(rows: np.ndarray, interactions: np.ndarray, base_mua, base_mus, comb
     combos: (C, 2L) array or CUDA tensor of (mua'_1..L, mus'_1..L);
     photons: N of the run.  Returns a float64 CUDA tensor of C reflectances."""
     import torch
-    lib = load_library()
-    _bind(lib)
-    dev = torch.device("cuda", device)
-    rows = np.asarray(rows, dtype=np.float32)
-    L = rows.shape[1] - 2
-    D = rows.shape[0]
-    pl = torch.from_numpy(np.ascontiguousarray(rows[:, 1:L + 1].T)).to(dev)
-    ni = torch.from_numpy(np.ascontiguousarray(np.asarray(interactions, np.float32).T)).to(dev)
-    w = torch.from_numpy(np.ascontiguousarray(rows[:, 0])).to(dev)
+    prep = Prepared(rows, interactions, device)
     if not torch.is_tensor(combos):
         combos = torch.from_numpy(np.asarray(combos, dtype=np.float32))
-    combos = combos.to(dev, torch.float32).contiguous()
-    Cn = combos.shape[0]
-    out = torch.empty(Cn, dtype=torch.float64, device=dev)
-    nbytes = int(lib.mcml_wmc_workspace_bytes(D, Cn))
-    ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
-    s = WmcSet(pl.data_ptr(), ni.data_ptr(), w.data_ptr(), D, L)
-    bm = (C.c_float * MAX_LAYERS)(*[float(v) for v in base_mua][:L])
-    bs = (C.c_float * MAX_LAYERS)(*[float(v) for v in base_mus][:L])
-    stream = torch.cuda.current_stream(dev).cuda_stream
-    _check(lib.mcml_wmc_rescale(C.byref(s), bm, bs, C.c_void_p(combos.data_ptr()), Cn,
-                                float(0xFFFFFFFF) * float(photons), C.c_void_p(out.data_ptr()),
-                                C.c_void_p(ws.data_ptr()), nbytes, C.c_void_p(stream)),
-           "mcml_wmc_rescale")
-    return out
+    combos = combos.to(torch.device("cuda", device), torch.float32).contiguous()
+    return prep.rescale(base_mua, base_mus, combos, photons)
 
 
 def rescale_reference(rows, interactions, base_mua, base_mus, combos, photons):
