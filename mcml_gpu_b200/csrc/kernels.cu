@@ -66,6 +66,9 @@ __device__ __forceinline__ void clear_gauss(curandStateXORWOW &st) {
 template <int kBlock>
 struct SeedStore {
   uint32_t w[6][kBlock];
+  // per-thread slot bookkeeping, touched only when a photon starts or ends
+  // or is detected, so it lives here instead of in registers
+  uint32_t slot[kBlock], k[kBlock], quota[kBlock], steps[kBlock];
   __device__ __forceinline__ void save(const curandStateXORWOW &st) {
     const int t = threadIdx.x;
     w[0][t] = st.d;
@@ -128,42 +131,37 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
     walk_kernel(const __grid_constant__ DevParams P, const WalkArgs A) {
   __shared__ SmemTables t;
   __shared__ SeedStore<kBlock> sc;
+  __shared__ uint64_t s_q, s_rem;  // photons per slot; slots with one more
+  if (threadIdx.x == 0) {
+    s_q = P.num_photons / P.num_slots;
+    s_rem = P.num_photons % P.num_slots;
+  }
   load_tables(t, P);
   __syncthreads();
-
-  const uint64_t S = P.num_slots;
-  const uint64_t q = P.num_photons / S;
-  const uint64_t rem = P.num_photons % S;
-  const int n_layers = (int)P.n_layers;
-  const int n_sds = (int)P.n_sds;
-  const float det_refl = P.det_reflectance;
-  const float start_w = P.start_weight;
+  const int tid = threadIdx.x;
 
   curandStateXORWOW st;
   clear_gauss(st);
   Photon p;
-  uint32_t slot = 0;   // current slot (S < 2^32)
-  uint32_t k = 0;      // ordinal of the current photon within its slot
-  uint32_t quota = 0;  // photons of the current slot
-  uint32_t steps_acc = 0;
+  sc.steps[tid] = 0;
 
   auto next_slot = [&]() -> bool {
     const uint64_t s = fetch_one(&A.counters[kCntSlot]);
     if (s >= A.slot_end) return false;
-    slot = (uint32_t)s;
+    sc.slot[tid] = (uint32_t)s;  // slots < 2^32
     load_state(st, A.slot_state, s);
-    k = 0;
-    quota = (uint32_t)(q + (s < rem ? 1 : 0));
+    sc.k[tid] = 0;
+    sc.quota[tid] = (uint32_t)(s_q + (s < s_rem ? 1 : 0));
     return true;
   };
   auto photon_index = [&]() -> uint64_t {
-    const uint64_t s = slot;
-    return s * q + (s < rem ? s : rem) + k;
+    const uint64_t s = sc.slot[tid];
+    return s * s_q + (s < s_rem ? s : s_rem) + sc.k[tid];
   };
 
   if (!next_slot()) return;
   sc.save(st);
-  launch_photon<kSrcOblique>(p, &st, t, start_w);
+  launch_photon<kSrcOblique>(p, &st, t, P.start_weight);
 
   for (;;) {
     // The photon's layer record, read once per step: hop, clamp and (when
@@ -181,7 +179,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
         if (new_layer == 0) {
           bool detected = false;
           if (kDetOblique) {
-            unsigned mask = fiber_mask(p, t, n_sds);
+            unsigned mask = fiber_mask(p, t, (int)P.n_sds);
             detected = mask != 0u;
             while (mask) {
               const int i = __ffs(mask) - 1;
@@ -191,7 +189,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
           } else {
             const float uz_angle = acosf(fabsf(p.dz));
             const float distance = radius_xy(p);
-            for (int i = 1; i <= n_sds; i++) {
+            for (int i = 1; i <= (int)P.n_sds; i++) {
               float wd;
               if (ring_hit(p, t, i, uz_angle, distance, wd)) {
                 append_record(A, photon_index(), i, wd, sc);
@@ -201,7 +199,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
           }
           if (detected) {
             p.w = 0;
-          } else if (uni(&st) > det_refl) {
+          } else if (uni(&st) > P.det_reflectance) {
             p.w = 0;
           } else {
             p.dz *= -1;
@@ -209,7 +207,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
             p.layer = temp_layer;
           }
         }
-        if (new_layer > n_layers) p.w = 0;
+        if (new_layer > (int)P.n_layers) p.w = 0;
       }
     }
 
@@ -219,14 +217,18 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
     }
 
     if (!survive<true>(p, &st)) {
-      steps_acc += (uint32_t)p.steps;  // steps of the photon that just ended
-      if (++k >= quota || steps_acc >= 0x40000000u) {
-        atomicAdd(&A.counters[kCntSteps], (unsigned long long)steps_acc);
-        steps_acc = 0;
+      const uint32_t acc = sc.steps[tid] + (uint32_t)p.steps;  // with the photon that just ended
+      const uint32_t kk = ++sc.k[tid];
+      const bool slot_done = kk >= sc.quota[tid];
+      if (slot_done || acc >= 0x40000000u) {
+        atomicAdd(&A.counters[kCntSteps], (unsigned long long)acc);
+        sc.steps[tid] = 0;
+      } else {
+        sc.steps[tid] = acc;
       }
-      if (k >= quota && !next_slot()) break;
+      if (slot_done && !next_slot()) break;
       sc.save(st);
-      launch_photon<kSrcOblique>(p, &st, t, start_w);
+      launch_photon<kSrcOblique>(p, &st, t, P.start_weight);
     }
   }
 }
