@@ -55,7 +55,7 @@ WORKLOAD = "plain MC + replay, 5-layer tissue, 1e8 photons, -R -A -B"
 # thread-instructions per clock (4 schedulers x 32 lanes) and 16 MUFU
 # results, so steps/s <= f_sm * 148 * min(128 / (98 + 9), 16 / 9): the
 # issue rate binds.  ncu's pipe counters agree that MUFU is not the limit:
-# 9.6 XU thread-instructions per step, 90 % of issue slots used.
+# 9.5 XU thread-instructions per step, 91 % of issue slots used.
 OPS_LANE = 98
 OPS_MUFU = 9
 SM_COUNT = 148
