@@ -79,13 +79,17 @@ struct GemmArgs {
   long long ldh, strideH;
   const float *aux;        // Zprev for kGeluBack
   long long ldx, strideX;
+  int splits, kper;        // kStoreF32: K split over gridDim.z (partial sums added atomically)
 };
 
 template <bool TA, bool TB, int EPI>
 __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(const GemmArgs g) {
   __shared__ __align__(16) bf16 As[BM][BK + PAD];
   __shared__ __align__(16) bf16 Bs[BK][BN + PAD];
-  const int z = blockIdx.z;
+  const int splits = g.splits > 1 ? g.splits : 1;
+  const int z = blockIdx.z / splits;  // ensemble member
+  const int k_begin = splits > 1 ? (int)(blockIdx.z % splits) * g.kper : 0;
+  const int k_end = splits > 1 ? min(g.K, k_begin + g.kper) : g.K;
   const bf16 *A = g.A + z * g.strideA;
   const bf16 *B = g.B + z * g.strideB;
   const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
@@ -99,7 +103,7 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(const GemmArgs g) {
 #pragma unroll
       for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.0f;
 
-  for (int k0 = 0; k0 < g.K; k0 += BK) {
+  for (int k0 = k_begin; k0 < k_end; k0 += BK) {
     // A tile: As[m][k] = op(A)(m0+m, k0+k); consecutive threads read
     // consecutive global addresses in either orientation.
     for (int e = tid; e < BM * BK; e += kGemmThreads) {
@@ -107,7 +111,7 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(const GemmArgs g) {
       if (TA) { m = e % BM; k = e / BM; } else { k = e % BK; m = e / BK; }
       const int gm = m0 + m, gk = k0 + k;
       bf16 v = __float2bfloat16(0.0f);
-      if (gm < g.M && gk < g.K) v = TA ? A[(long long)gk * g.lda + gm] : A[(long long)gm * g.lda + gk];
+      if (gm < g.M && gk < k_end) v = TA ? A[(long long)gk * g.lda + gm] : A[(long long)gm * g.lda + gk];
       As[m][k] = v;
     }
     for (int e = tid; e < BK * BN; e += kGemmThreads) {
@@ -115,7 +119,7 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(const GemmArgs g) {
       if (TB) { k = e % BK; n = e / BK; } else { n = e % BN; k = e / BN; }
       const int gk = k0 + k, gn = n0 + n;
       bf16 v = __float2bfloat16(0.0f);
-      if (gk < g.K && gn < g.N) v = TB ? B[(long long)gn * g.ldb + gk] : B[(long long)gk * g.ldb + gn];
+      if (gk < k_end && gn < g.N) v = TB ? B[(long long)gn * g.ldb + gk] : B[(long long)gk * g.ldb + gn];
       Bs[k][n] = v;
     }
     __syncthreads();
@@ -164,7 +168,11 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(const GemmArgs g) {
         if (m >= g.M || n >= g.N) continue;
         const float v = acc[i][j][r];
         if (EPI == kStoreF32) {
-          g.outF[z * g.strideO + (long long)m * g.ldo + n] = v;
+          float *o = &g.outF[z * g.strideO + (long long)m * g.ldo + n];
+          if (splits > 1)
+            atomicAdd(o, v);
+          else
+            *o = v;
         } else {  // kGeluBack
           const float zp = g.aux[z * g.strideX + (long long)m * g.ldx + n];
           g.outH[z * g.strideH + (long long)m * g.ldh + n] = __float2bfloat16(v * gelu_grad(zp));
@@ -174,7 +182,7 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(const GemmArgs g) {
 
 template <bool TA, bool TB, int EPI>
 cudaError_t gemm(const GemmArgs &g, int members, cudaStream_t s) {
-  dim3 grid((g.N + BN - 1) / BN, (g.M + BM - 1) / BM, members);
+  dim3 grid((g.N + BN - 1) / BN, (g.M + BM - 1) / BM, members * (g.splits > 1 ? g.splits : 1));
   gemm_kernel<TA, TB, EPI><<<grid, kGemmThreads, 0, s>>>(g);
   return cudaGetLastError();
 }
@@ -198,14 +206,20 @@ constexpr int TCM = 128;            // rows per tile (UMMA M)
 constexpr int kLboA = (TCM / 8) * 128;
 constexpr long long kTcSpin = 1ll << 22;
 
-enum TcEpi { kTcBiasGelu = 0, kTcBias = 1 };
+enum TcEpi {
+  kTcBiasGelu = 0,  // H = bf16(gelu(acc + b)), Z = acc + b (optional)
+  kTcBias = 1,      // Y = acc + b (FP32, the output layer)
+  kTcGeluBack = 2   // H = bf16(acc * gelu'(aux)) (back through an activation)
+};
 
 struct TcArgs {
   int M, N, K, n_valid;     // N: MMA width (multiple of 16); n_valid <= N real columns
   const bf16 *A;            // M x K, row-major, lda
   long long lda, strideA;
-  const bf16 *W;            // K x n_valid, row-major (ldw = n_valid)
+  const bf16 *W;            // K x n_valid row-major (B MN-major), or N x K row-major (B K-major)
   long long strideW;
+  const float *aux;         // kTcGeluBack: the pre-activations Z of the layer below
+  long long ldaux, strideAux;
   const float *bias;
   long long strideBias;
   float *Z;                 // kTcBiasGelu: pre-activations (may be null); kTcBias: output
@@ -278,6 +292,21 @@ __device__ __forceinline__ void epilogue32(const TcArgs &g, const uint32_t (&v)[
       for (int i = 0; i < 4; ++i) h[i] = __floats2bfloat162_rn(gelu(f[2 * i]), gelu(f[2 * i + 1]));
       hrow[b] = *reinterpret_cast<const uint4 *>(h);
     }
+  } else if (EPI == kTcGeluBack) {
+    const float4 *zrow =
+        reinterpret_cast<const float4 *>(g.aux + z * g.strideAux + (long long)row * g.ldaux + c0);
+    uint4 *hrow = reinterpret_cast<uint4 *>(g.H + z * g.strideH + (long long)row * g.ldh + c0);
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const float4 z0 = zrow[2 * b], z1 = zrow[2 * b + 1];
+      const float zp[8] = {z0.x, z0.y, z0.z, z0.w, z1.x, z1.y, z1.z, z1.w};
+      __align__(16) __nv_bfloat162 h[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        h[i] = __floats2bfloat162_rn(__uint_as_float(v[b * 8 + 2 * i]) * gelu_grad(zp[2 * i]),
+                                     __uint_as_float(v[b * 8 + 2 * i + 1]) * gelu_grad(zp[2 * i + 1]));
+      hrow[b] = *reinterpret_cast<const uint4 *>(h);
+    }
   } else {
     float *y = g.Z + z * g.strideZ + (long long)row * g.ldz;
 #pragma unroll
@@ -310,7 +339,7 @@ __device__ __forceinline__ void umma_commit(uint32_t bar) {
 constexpr int kTcWarps = 12;
 constexpr int kProducers = 96;  // warps 0-2
 
-template <int EPI>
+template <int EPI, bool kBK>
 __global__ void __launch_bounds__(kTcWarps * 32, 1) tc_layer_kernel(const TcArgs g) {
   extern __shared__ __align__(1024) unsigned char smem[];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -355,7 +384,18 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1) tc_layer_kernel(const TcArgs
   }
   // The layer's weights and bias, once per CTA, by all warps.
   const bf16 *W = g.W + z * g.strideW;
-  if (g.n_valid == N) {
+  if (kBK) {
+    // B K-major from W (N x K, row-major): element (n, k) at
+    // (k/8)*lboB + (n/8)*128 + (n%8)*16 + (k%8)*2, n % 8 fastest per 8 lanes
+    const int kc8 = K / 8;
+    for (int c = tid; c < N * kc8; c += kTcWarps * 32) {
+      const int n_lo = c & 7, rest = c >> 3;
+      const int kc = rest % kc8, n = (rest / kc8) * 8 + n_lo;
+      const uint32_t dst = sB_u + kc * lboB + (n >> 3) * 128 + n_lo * 16;
+      const bf16 *src = W + (long long)n * K + kc * 8;
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
+    }
+  } else if (g.n_valid == N) {
     const int nc8 = N / 8;
     for (int c = tid; c < K * nc8; c += kTcWarps * 32) {
       const int k_lo = c & 7, rest = c >> 3;
@@ -372,8 +412,9 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1) tc_layer_kernel(const TcArgs
       sb[((k >> 3) * lboB + (n >> 3) * 128 + (k & 7) * 16 + (n & 7) * 2) / 2] = v;
     }
   }
-  const float *bias = g.bias + z * g.strideBias;
-  for (int n = tid; n < N; n += kTcWarps * 32) sBias[n] = n < g.n_valid ? bias[n] : 0.0f;
+  const float *bias = g.bias ? g.bias + z * g.strideBias : nullptr;
+  for (int n = tid; n < N; n += kTcWarps * 32)
+    sBias[n] = (g.bias && n < g.n_valid) ? bias[n] : 0.0f;
   asm volatile("cp.async.wait_all;\n" ::: "memory");
   asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
@@ -421,7 +462,8 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1) tc_layer_kernel(const TcArgs
   } else if (warp == 3) {
     // ---- MMA issuer
     if (lane == 0) {
-      const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (0u << 15) | (1u << 16) |
+      const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (0u << 15) |
+                             ((kBK ? 0u : 1u) << 16) |  // B: K-major or MN-major
                              ((uint32_t)(N >> 3) << 17) | ((uint32_t)(TCM >> 4) << 24);
       int t = 0;
       for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++t) {
@@ -503,7 +545,14 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1) tc_layer_kernel(const TcArgs
           float f[8];
 #pragma unroll
           for (int i = 0; i < 8; ++i) f[i] = __uint_as_float(v[i]) + sBias[c0 + i];
-          if (EPI == kTcBiasGelu) {
+          if (EPI == kTcGeluBack) {
+            const float *zp = g.aux + z * g.strideAux + (long long)row * g.ldaux + c0;
+            __align__(16) bf16 h[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) h[i] = __float2bfloat16(__uint_as_float(v[i]) * gelu_grad(zp[i]));
+            *reinterpret_cast<uint4 *>(g.H + z * g.strideH + (long long)row * g.ldh + c0) =
+                *reinterpret_cast<const uint4 *>(h);
+          } else if (EPI == kTcBiasGelu) {
             if (g.Z) {
               float4 *zp = reinterpret_cast<float4 *>(g.Z + z * g.strideZ + (long long)row * g.ldz + c0);
               zp[0] = make_float4(f[0], f[1], f[2], f[3]);
@@ -554,7 +603,7 @@ size_t tc_smem_bytes(int K, int N, int slots) {
   return std::max<size_t>(need, 120 * 1024);
 }
 
-template <int EPI>
+template <int EPI, bool kBK = false>
 cudaError_t tc_layer(const TcArgs &g, int members, cudaStream_t s) {
   if (g.N % 16 || g.N < 16 || g.N > 256 || g.K % 16 || g.K < 16 || g.K > 256 || g.n_valid > g.N)
     return cudaErrorInvalidValue;
@@ -568,7 +617,7 @@ cudaError_t tc_layer(const TcArgs &g, int members, cudaStream_t s) {
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
   if (!configured[dev]) {
-    e = cudaFuncSetAttribute(tc_layer_kernel<EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(tc_layer_kernel<EPI, kBK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)kTcSmemMax);
     if (e != cudaSuccess) return e;
     configured[dev] = true;
@@ -583,7 +632,7 @@ cudaError_t tc_layer(const TcArgs &g, int members, cudaStream_t s) {
   const int tiles = (g.M + TCM - 1) / TCM;
   const int per_member = std::max(1, sms[dev] / std::max(1, members));
   dim3 grid(std::min(tiles, per_member), 1, members);
-  tc_layer_kernel<EPI><<<grid, kTcWarps * 32, smem, s>>>(a);
+  tc_layer_kernel<EPI, kBK><<<grid, kTcWarps * 32, smem, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -827,6 +876,11 @@ int check_status(mcml_mlp *p) {
 // Backward from dY (in d_dy, BF16) to all weight/bias gradients in d_g.
 int backward(mcml_mlp *p, int n) {
   const long long H = p->hidden, cap = p->cap, P = p->stride, D = p->depth;
+  // dW = X^T dZ runs over the batch: split it so that a few layers of
+  // 256 x 256 still fill the GPU, partial sums added atomically into d_g
+  const int splits = std::max(1, std::min(16, n / 256));
+  const int kper = ((n + splits - 1) / splits + BK - 1) / BK * BK;
+  if (splits > 1) MLP_TRY(cudaMemsetAsync(p->d_g, 0, p->E * P * sizeof(float), p->stream));
   bf16 *dcur = p->d_dy;   // gradient w.r.t. the current layer's output (pre-activation)
   bf16 *dnext = p->d_dh;
   long long dcur_ld = p->out_dim;
@@ -853,13 +907,42 @@ int backward(mcml_mlp *p, int n) {
     g.outF = p->d_g + p->w_off[l];
     g.ldo = fo;
     g.strideO = P;
+    // the batch dimension split over blocks (d_g zeroed above)
+    g.splits = splits;
+    g.kper = kper;
     MLP_TRY((gemm<true, false, kStoreF32>(g, p->E, p->stream)));
     // db_l = column sums of dZ_l
     bias_grad_kernel<<<dim3((fo + 127) / 128, 1, p->E), 128, 0, p->stream>>>(
         dcur, cap * std::max<long long>(H, p->out_dim), n, fo, p->d_g + p->b_off[l], P);
     MLP_TRY(cudaGetLastError());
     if (l == 0) break;
-    // dZ_{l-1} = (dZ_l W_l^T) * gelu'(Z_{l-1})   (M = n, N = fi, K = fo)
+    // dZ_{l-1} = (dZ_l W_l^T) * gelu'(Z_{l-1})   (M = n, N = fi, K = fo):
+    // on the tensor cores (W_l as a K-major B operand) when fo is a hidden
+    // width; the output layer's narrow fo stays on the mma.sync kernel
+    if (fo % 16 == 0) {
+      TcArgs t;
+      std::memset(&t, 0, sizeof(t));
+      t.M = n;
+      t.N = fi;
+      t.n_valid = fi;
+      t.K = fo;
+      t.A = dcur;
+      t.lda = dcur_ld;
+      t.strideA = cap * std::max<long long>(H, p->out_dim);
+      t.W = p->d_w16 + p->w_off[l];
+      t.strideW = P;
+      t.aux = p->d_z + (long long)(l - 1) * cap * H;
+      t.ldaux = H;
+      t.strideAux = D * cap * H;
+      t.H = dnext;
+      t.ldh = H;
+      t.strideH = cap * std::max<long long>(H, p->out_dim);
+      t.status = p->d_status;
+      MLP_TRY((tc_layer<kTcGeluBack, true>(t, p->E, p->stream)));
+      std::swap(dcur, dnext);
+      dcur_ld = H;
+      continue;
+    }
     GemmArgs b;
     std::memset(&b, 0, sizeof(b));
     b.M = n;

@@ -68,9 +68,10 @@ def cpu_reference(params, shapes, X, T, xm, xs, tm, ts):
 
 
 @pytest.mark.gpu
-def test_gradients_match_cpu_reference(gpu_available):
+@pytest.mark.parametrize("n", [192, 1024])  # 1024: the weight gradients split over the batch
+def test_gradients_match_cpu_reference(n, gpu_available):
     rng = np.random.default_rng(0)
-    n, in_dim, out_dim = 192, 25, 3
+    in_dim, out_dim = 25, 3
     X = rng.normal(size=(n, in_dim)).astype(np.float32) * 2 + 1
     T = rng.normal(size=(n, out_dim)).astype(np.float32) * 3 - 2
     mlp = sg.MLP(in_dim, out_dim, hidden=64, depth=3, ensemble=2, seed=5)
