@@ -10,6 +10,10 @@
 // tensor cores (operands in shared memory, FP32 accumulator in tensor
 // memory, bias + GELU epilogue from tcgen05.ld).
 //
+// Backward: the hidden layers' dH = (dZ W^T) * gelu'(Z) on tc_layer_kernel
+// (weights as a K-major B operand); the weight gradients and the output
+// layer's narrow dH on the GEMM below.
+//
 // Backward GEMM: C[M x N] = op(A)[M x K] * op(B)[K x N], BF16 operands staged in
 // shared memory, mma.sync m16n8k16 fragments loaded with ldmatrix, FP32
 // accumulators, and a fused epilogue:
