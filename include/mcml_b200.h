@@ -313,9 +313,9 @@ int mcml_wmc_rescale(const mcml_wmc_set *set, const float *base_mua, const float
  * No counterpart in the reference.  An ensemble of MLPs
  * (in -> hidden x depth, GELU -> out) trained and evaluated by this
  * library's BF16 tensor-core kernels with FP32 accumulation and FP32
- * master weights (Adam): the forward pass and the hidden layers' input
- * gradients on tcgen05 (accumulators in tensor memory), the weight
- * gradients on mma.sync.  Limits: in_dim and
+ * master weights (Adam), forward and backward products on tcgen05
+ * (accumulators in tensor memory; the output layer's 3-wide input
+ * gradient on mma.sync).  Limits: in_dim and
  * hidden at most 256, hidden a multiple of 16, out_dim <= hidden.  Inputs and targets are normalised with
  * mcml_mlp_set_normalization; predictions come back de-normalised with the
  * ensemble's spread.  X, T, mean and spread are DEVICE arrays.

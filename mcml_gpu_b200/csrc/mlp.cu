@@ -213,7 +213,8 @@ constexpr long long kTcSpin = 1ll << 22;
 enum TcEpi {
   kTcBiasGelu = 0,  // H = bf16(gelu(acc + b)), Z = acc + b (optional)
   kTcBias = 1,      // Y = acc + b (FP32, the output layer)
-  kTcGeluBack = 2   // H = bf16(acc * gelu'(aux)) (back through an activation)
+  kTcGeluBack = 2,  // H = bf16(acc * gelu'(aux)) (back through an activation)
+  kTcAddF32 = 3     // Z += acc (FP32 atomics: partial sums of a split K)
 };
 
 struct TcArgs {
@@ -232,6 +233,8 @@ struct TcArgs {
   long long ldh, strideH;
   unsigned *status;
   int slots;                // A ring slots (chunks of up to 64 K columns), 2..16
+  int splits;               // K split over gridDim.z (member = z / splits, slice = z % splits)
+  long long sliceA, sliceW; // element offsets of one K slice in A and W
 };
 
 __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
@@ -311,6 +314,11 @@ __device__ __forceinline__ void epilogue32(const TcArgs &g, const uint32_t (&v)[
                                      __uint_as_float(v[b * 8 + 2 * i + 1]) * gelu_grad(zp[2 * i + 1]));
       hrow[b] = *reinterpret_cast<const uint4 *>(h);
     }
+  } else if (EPI == kTcAddF32) {
+    float *y = g.Z + z * g.strideZ + (long long)row * g.ldz;
+#pragma unroll
+    for (int i = 0; i < 32; ++i)
+      if (c0 + i < g.n_valid) atomicAdd(&y[c0 + i], __uint_as_float(v[i]));
   } else {
     float *y = g.Z + z * g.strideZ + (long long)row * g.ldz;
 #pragma unroll
@@ -343,11 +351,13 @@ __device__ __forceinline__ void umma_commit(uint32_t bar) {
 constexpr int kTcWarps = 12;
 constexpr int kProducers = 96;  // warps 0-2
 
-template <int EPI, bool kBK>
+template <int EPI, bool kBK, bool kAMN>
 __global__ void __launch_bounds__(kTcWarps * 32, 1) tc_layer_kernel(const TcArgs g) {
   extern __shared__ __align__(1024) unsigned char smem[];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int z = blockIdx.z;
+  const int splits = g.splits > 1 ? g.splits : 1;
+  const int z = blockIdx.z / splits;      // ensemble member
+  const int slice = blockIdx.z % splits;  // K slice
   const int K = g.K, N = g.N;
   const int tiles = (g.M + TCM - 1) / TCM;
   const int KC = K < 64 ? K : 64;  // K per chunk
@@ -387,7 +397,7 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1) tc_layer_kernel(const TcArgs
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
   }
   // The layer's weights and bias, once per CTA, by all warps.
-  const bf16 *W = g.W + z * g.strideW;
+  const bf16 *W = g.W + z * g.strideW + slice * g.sliceW;
   if (kBK) {
     // B K-major from W (N x K, row-major): element (n, k) at
     // (k/8)*lboB + (n/8)*128 + (n%8)*16 + (k%8)*2, n % 8 fastest per 8 lanes
@@ -425,7 +435,7 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1) tc_layer_kernel(const TcArgs
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   const uint32_t tmem = *tslot;
-  const bf16 *A = g.A + z * g.strideA;
+  const bf16 *A = g.A + z * g.strideA + slice * g.sliceA;
 
   if (warp < 3) {
     // ---- producers: A chunks into the ring.  Each thread's copies of a
@@ -447,16 +457,33 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1) tc_layer_kernel(const TcArgs
           break;
         }
         const uint32_t base = sA_u + (uint32_t)slot * slot_bytes;
-        for (int e = tid; e < per_chunk; e += kProducers) {
-          const int r_lo = e & 7, rest = e >> 3;
-          const int kl = rest % (KC / 8), r = (rest / (KC / 8)) * 8 + r_lo;
-          const uint32_t dst = base + kl * kLboA + (r >> 3) * 128 + r_lo * 16;
-          const int gr = m0 + r;
-          const bf16 *src = A + (long long)(gr < g.M ? gr : 0) * g.lda + (c * (KC / 8) + kl) * 8;
-          const uint32_t bytes = gr < g.M ? 16u : 0u;
-          asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src),
-                       "r"(bytes)
-                       : "memory");
+        if (kAMN) {
+          // A MN-major from a K x M row-major array (A(m, k) at A[k*lda + m]):
+          // element (m, k) at (k/8)*kLboA + (m/8)*128 + (k%8)*16 + (m%8)*2
+          for (int e = tid; e < per_chunk; e += kProducers) {
+            const int k_lo = e & 7, rest = e >> 3;
+            const int mc = rest % (TCM / 8), kg = rest / (TCM / 8);
+            const uint32_t dst = base + kg * kLboA + mc * 128 + k_lo * 16;
+            const int gm = m0 + mc * 8;
+            const int gk = c * KC + kg * 8 + k_lo;
+            const bf16 *src = A + (long long)gk * g.lda + (gm < g.M ? gm : 0);
+            const uint32_t bytes = gm < g.M ? 16u : 0u;
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src),
+                         "r"(bytes)
+                         : "memory");
+          }
+        } else {
+          for (int e = tid; e < per_chunk; e += kProducers) {
+            const int r_lo = e & 7, rest = e >> 3;
+            const int kl = rest % (KC / 8), r = (rest / (KC / 8)) * 8 + r_lo;
+            const uint32_t dst = base + kl * kLboA + (r >> 3) * 128 + r_lo * 16;
+            const int gr = m0 + r;
+            const bf16 *src = A + (long long)(gr < g.M ? gr : 0) * g.lda + (c * (KC / 8) + kl) * 8;
+            const uint32_t bytes = gr < g.M ? 16u : 0u;
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src),
+                         "r"(bytes)
+                         : "memory");
+          }
         }
         asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(a_full(slot))
                      : "memory");
@@ -466,8 +493,9 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1) tc_layer_kernel(const TcArgs
   } else if (warp == 3) {
     // ---- MMA issuer
     if (lane == 0) {
-      const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (0u << 15) |
-                             ((kBK ? 0u : 1u) << 16) |  // B: K-major or MN-major
+      const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) |
+                             ((kAMN ? 1u : 0u) << 15) |  // A: MN-major or K-major
+                             ((kBK ? 0u : 1u) << 16) |   // B: K-major or MN-major
                              ((uint32_t)(N >> 3) << 17) | ((uint32_t)(TCM >> 4) << 24);
       int t = 0;
       for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++t) {
@@ -549,7 +577,12 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1) tc_layer_kernel(const TcArgs
           float f[8];
 #pragma unroll
           for (int i = 0; i < 8; ++i) f[i] = __uint_as_float(v[i]) + sBias[c0 + i];
-          if (EPI == kTcGeluBack) {
+          if (EPI == kTcAddF32) {
+            float *y = g.Z + z * g.strideZ + (long long)row * g.ldz;
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+              if (c0 + i < g.n_valid) atomicAdd(&y[c0 + i], __uint_as_float(v[i]));
+          } else if (EPI == kTcGeluBack) {
             const float *zp = g.aux + z * g.strideAux + (long long)row * g.ldaux + c0;
             __align__(16) bf16 h[8];
 #pragma unroll
@@ -607,7 +640,7 @@ size_t tc_smem_bytes(int K, int N, int slots) {
   return std::max<size_t>(need, 120 * 1024);
 }
 
-template <int EPI, bool kBK = false>
+template <int EPI, bool kBK = false, bool kAMN = false>
 cudaError_t tc_layer(const TcArgs &g, int members, cudaStream_t s) {
   if (g.N % 16 || g.N < 16 || g.N > 256 || g.K % 16 || g.K < 16 || g.K > 256 || g.n_valid > g.N)
     return cudaErrorInvalidValue;
@@ -621,7 +654,7 @@ cudaError_t tc_layer(const TcArgs &g, int members, cudaStream_t s) {
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
   if (!configured[dev]) {
-    e = cudaFuncSetAttribute(tc_layer_kernel<EPI, kBK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(tc_layer_kernel<EPI, kBK, kAMN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)kTcSmemMax);
     if (e != cudaSuccess) return e;
     configured[dev] = true;
@@ -634,9 +667,10 @@ cudaError_t tc_layer(const TcArgs &g, int members, cudaStream_t s) {
   // persistent: one CTA per SM shared out among the members, each CTA
   // walking its member's 128-row tiles with the weights resident
   const int tiles = (g.M + TCM - 1) / TCM;
-  const int per_member = std::max(1, sms[dev] / std::max(1, members));
-  dim3 grid(std::min(tiles, per_member), 1, members);
-  tc_layer_kernel<EPI, kBK><<<grid, kTcWarps * 32, smem, s>>>(a);
+  const int zs = std::max(1, members) * std::max(1, g.splits);
+  const int per_z = std::max(1, sms[dev] / zs);
+  dim3 grid(std::min(tiles, per_z), 1, zs);
+  tc_layer_kernel<EPI, kBK, kAMN><<<grid, kTcWarps * 32, smem, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -884,13 +918,37 @@ int backward(mcml_mlp *p, int n) {
   // 256 x 256 still fill the GPU, partial sums added atomically into d_g
   const int splits = std::max(1, std::min(16, n / 256));
   const int kper = ((n + splits - 1) / splits + BK - 1) / BK * BK;
-  if (splits > 1) MLP_TRY(cudaMemsetAsync(p->d_g, 0, p->E * P * sizeof(float), p->stream));
+  MLP_TRY(cudaMemsetAsync(p->d_g, 0, p->E * P * sizeof(float), p->stream));
+  // with whole slices of 256 rows the weight gradients run on the tensor
+  // cores: one slice per CTA group, A = X_l^T read MN-major from X_l
+  const bool tc_dw = n % 256 == 0;
   bf16 *dcur = p->d_dy;   // gradient w.r.t. the current layer's output (pre-activation)
   bf16 *dnext = p->d_dh;
   long long dcur_ld = p->out_dim;
   for (int l = p->layers - 1; l >= 0; --l) {
     const int fo = p->fan_out[l], fi = p->fan_in[l];
     // dW_l = X_l^T dZ_l  (M = fi, N = fo, K = n)
+    if (tc_dw) {
+      TcArgs w;
+      std::memset(&w, 0, sizeof(w));
+      w.M = fi;
+      w.N = (fo + 15) / 16 * 16;
+      w.n_valid = fo;
+      w.K = 256;
+      w.A = l == 0 ? p->d_x : p->d_h + (long long)(l - 1) * cap * H;
+      w.lda = l == 0 ? p->in_pad : H;
+      w.strideA = l == 0 ? cap * p->in_pad : D * cap * H;
+      w.sliceA = 256 * w.lda;
+      w.W = dcur;
+      w.strideW = cap * std::max<long long>(H, p->out_dim);
+      w.sliceW = 256 * dcur_ld;
+      w.Z = p->d_g + p->w_off[l];
+      w.ldz = fo;
+      w.strideZ = P;
+      w.splits = n / 256;
+      w.status = p->d_status;
+      MLP_TRY((tc_layer<kTcAddF32, false, true>(w, p->E, p->stream)));
+    } else {
     GemmArgs g;
     std::memset(&g, 0, sizeof(g));
     g.M = fi;
@@ -915,6 +973,7 @@ int backward(mcml_mlp *p, int n) {
     g.splits = splits;
     g.kper = kper;
     MLP_TRY((gemm<true, false, kStoreF32>(g, p->E, p->stream)));
+    }
     // db_l = column sums of dZ_l
     bias_grad_kernel<<<dim3((fo + 127) / 128, 1, p->E), 128, 0, p->stream>>>(
         dcur, cap * std::max<long long>(H, p->out_dim), n, fo, p->d_g + p->b_off[l], P);
