@@ -11,8 +11,10 @@
 // memory, bias + GELU epilogue from tcgen05.ld).
 //
 // Backward: the hidden layers' dH = (dZ W^T) * gelu'(Z) on tc_layer_kernel
-// (weights as a K-major B operand); the weight gradients and the output
-// layer's narrow dH on the GEMM below.
+// (weights as a K-major B operand) and the weight gradients dW = X^T dZ
+// (X as an MN-major A operand, 256-row batch slices added atomically); the
+// output layer's 3-wide dH, and dW of batches that are not whole slices,
+// on the GEMM below.
 //
 // Backward GEMM: C[M x N] = op(A)[M x K] * op(B)[K x N], BF16 operands staged in
 // shared memory, mma.sync m16n8k16 fragments loaded with ldmatrix, FP32
