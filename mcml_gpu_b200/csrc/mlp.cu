@@ -23,6 +23,7 @@
 //   kStoreF32 : G = acc (FP32; weight gradients)
 // op(A) = A or A^T, op(B) = B or B^T by template flags, which gives the
 // backward products dW = H^T dZ and dH = dZ W^T from the same kernel.
+#include <cuda.h>  // CUtensorMap (the encoder is reached through the runtime)
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -237,6 +238,7 @@ struct TcArgs {
   int slots;                // A ring slots (chunks of up to 64 K columns), 2..16
   int splits;               // K split over gridDim.z (member = z / splits, slice = z % splits)
   long long sliceA, sliceW; // element offsets of one K slice in A and W
+  int use_tma;              // A chunks by TMA, 128-byte swizzled (K-major A, K % 64 == 0)
 };
 
 __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
@@ -246,6 +248,20 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint
   d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
   d |= (uint64_t)1 << 46;  // descriptor version (Blackwell)
   return d;                // base offset 0, no swizzle
+}
+
+// K-major operand as TMA writes it with 128-byte swizzling: rows of 128 B
+// (64 BF16), 8-row groups 1024 B apart (SBO), the two 16-byte K halves of
+// an MMA adjacent (LBO field 1); K steps within the 128-byte atom advance
+// the start address by 32 B.  The tile base must be 1024-byte aligned.
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+  d |= (uint64_t)1 << 16;             // LBO: 16 B
+  d |= (uint64_t)(1024 >> 4) << 32;   // SBO: 1024 B
+  d |= (uint64_t)1 << 46;             // descriptor version (Blackwell)
+  d |= (uint64_t)2 << 61;             // 128-byte swizzle
+  return d;
 }
 
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
@@ -354,8 +370,11 @@ constexpr int kTcWarps = 12;
 constexpr int kProducers = 96;  // warps 0-2
 
 template <int EPI, bool kBK, bool kAMN>
-__global__ void __launch_bounds__(kTcWarps * 32, 1) tc_layer_kernel(const TcArgs g) {
-  extern __shared__ __align__(1024) unsigned char smem[];
+__global__ void __launch_bounds__(kTcWarps * 32, 1)
+    tc_layer_kernel(const TcArgs g, const __grid_constant__ CUtensorMap tmA) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  // 1024-byte aligned base (the swizzled A tiles need it)
+  unsigned char *smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int splits = g.splits > 1 ? g.splits : 1;
   const int z = blockIdx.z / splits;      // ensemble member
@@ -367,8 +386,9 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1) tc_layer_kernel(const TcArgs
   const int nslots = g.slots;      // A ring: chunk i of the CTA's sequence uses slot i % nslots
   const uint32_t slot_bytes = (uint32_t)(KC / 8) * kLboA;
   const uint32_t lboB = (uint32_t)(N / 8) * 128;
+  const bool tma = g.use_tma != 0;
   unsigned char *sB = smem;
-  unsigned char *sA = smem + (size_t)K * N * 2;
+  unsigned char *sA = smem + (((size_t)K * N * 2 + 1023) & ~(size_t)1023);
   float *sBias = reinterpret_cast<float *>(sA + (size_t)nslots * slot_bytes);
   uint64_t *bars = reinterpret_cast<uint64_t *>(sBias + 256);
   uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 36);
@@ -382,7 +402,7 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1) tc_layer_kernel(const TcArgs
 
   if (tid == 0) {
     for (int c = 0; c < nslots; ++c) {
-      mbar_init(a_full(c), kProducers);
+      mbar_init(a_full(c), tma ? 1 : kProducers);
       mbar_init(a_empty(c), 1);
     }
     for (int b = 0; b < 2; ++b) {
@@ -439,7 +459,36 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1) tc_layer_kernel(const TcArgs
   const uint32_t tmem = *tslot;
   const bf16 *A = g.A + z * g.strideA + slice * g.sliceA;
 
-  if (warp < 3) {
+  if (warp < 3 && tma) {
+    // ---- producer (one thread): each A chunk is one TMA box of 64 K x 128
+    // rows, 128-byte swizzled, counted on a_full by its byte total; rows
+    // past M read as zeros.  Coordinates: (K offset, row, member).
+    if (tid == 0) {
+      int gi = 0;
+      bool alive = true;
+      for (int tile = blockIdx.x; tile < tiles && alive; tile += gridDim.x) {
+        for (int c = 0; c < nch; ++c, ++gi) {
+          const int slot = gi % nslots, use = gi / nslots;
+          if (use > 0 && !mbar_wait(a_empty(slot), (uint32_t)((use - 1) & 1))) {
+            atomicOr(g.status, 1u);
+            alive = false;
+            break;
+          }
+          const uint32_t dst = sA_u + (uint32_t)slot * slot_bytes;
+          asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(a_full(slot)),
+                       "r"(slot_bytes)
+                       : "memory");
+          asm volatile(
+              "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+              " [%0], [%1, {%3, %4, %5}], [%2];\n" ::"r"(dst),
+              "l"(reinterpret_cast<uint64_t>(&tmA)), "r"(a_full(slot)), "r"(c * KC),
+              "r"(tile * TCM), "r"(z)
+              : "memory");
+        }
+      }
+    }
+    __syncwarp();
+  } else if (warp < 3) {
     // ---- producers: A chunks into the ring.  Each thread's copies of a
     // chunk arrive on a_full[slot] by themselves when they land
     // (cp.async.mbarrier.arrive.noinc; the barrier expects all 96 producer
@@ -520,7 +569,8 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1) tc_layer_kernel(const TcArgs
           const uint32_t base = sA_u + (uint32_t)slot * slot_bytes;
           for (int j = 0; j < KC / 16; ++j) {
             const int ks = c * (KC / 16) + j;  // K step of 16 within the tile
-            const uint64_t ad = umma_desc(base + 2 * j * kLboA, kLboA, 128);
+            const uint64_t ad = tma ? umma_desc_sw128(base + 32 * j)
+                                    : umma_desc(base + 2 * j * kLboA, kLboA, 128);
             const uint64_t bd = umma_desc(sB_u + 2 * ks * lboB, lboB, 128);
             const uint32_t acc = ks > 0 ? 1u : 0u;
             asm volatile(
@@ -630,16 +680,61 @@ constexpr size_t kTcSmemFixed = 256 * 4 + 36 * 8 + 16;  // bias, barriers, TMEM 
 size_t tc_slot_bytes(int K) { return (size_t)(K < 64 ? K : 64) / 8 * kLboA; }
 
 // A ring slots: as many as fit beside the weights (at most 16).
+size_t tc_align1k(size_t n) { return (n + 1023) & ~(size_t)1023; }
+
+// A ring slots: as many as fit beside the weights (at most 16).
 int tc_slots(int K, int N) {
-  const size_t room = kTcSmemMax - (size_t)K * N * 2 - kTcSmemFixed;
+  const size_t room = kTcSmemMax - tc_align1k((size_t)K * N * 2) - kTcSmemFixed - 1024;
   return (int)std::min<size_t>(16, room / tc_slot_bytes(K));
 }
 
 size_t tc_smem_bytes(int K, int N, int slots) {
-  // at least 120 KB so that one CTA runs per SM and its tensor-memory
-  // allocation never waits for another's
-  const size_t need = (size_t)K * N * 2 + (size_t)slots * tc_slot_bytes(K) + kTcSmemFixed;
+  // weights, A ring, bias + barriers, 1 KB of alignment slack; at least
+  // 120 KB so that one CTA runs per SM and its tensor-memory allocation
+  // never waits for another's
+  const size_t need = tc_align1k((size_t)K * N * 2) + (size_t)slots * tc_slot_bytes(K) +
+                      kTcSmemFixed + 1024;
   return std::max<size_t>(need, 120 * 1024);
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                  const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                  const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no
+// link-time dependency on the driver library); null if unavailable.
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void *ptr = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(ptr);
+    else
+      cudaGetLastError();
+  }
+  return fn;
+}
+
+// Tensor map of A as (K, rows, member) for 64 x 128 boxes with 128-byte
+// swizzling.  False when A cannot be described (the caller then streams A
+// with cp.async).
+bool encode_a_map(const TcArgs &g, int members, CUtensorMap *map) {
+  EncodeTiledFn fn = encode_tiled();
+  if (!fn || g.K % 64 != 0) return false;
+  const cuuint64_t dims[3] = {(cuuint64_t)g.K, (cuuint64_t)g.M, (cuuint64_t)members};
+  const cuuint64_t strides[2] = {(cuuint64_t)g.lda * 2, (cuuint64_t)g.strideA * 2};
+  const cuuint32_t box[3] = {64, TCM, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  if (strides[0] % 16 || (members > 1 && strides[1] % 16) || ((uintptr_t)g.A & 15)) return false;
+  return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<bf16 *>(g.A), dims, strides, box,
+            estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 template <int EPI, bool kBK = false, bool kAMN = false>
@@ -672,7 +767,10 @@ cudaError_t tc_layer(const TcArgs &g, int members, cudaStream_t s) {
   const int zs = std::max(1, members) * std::max(1, g.splits);
   const int per_z = std::max(1, sms[dev] / zs);
   dim3 grid(std::min(tiles, per_z), 1, zs);
-  tc_layer_kernel<EPI, kBK, kAMN><<<grid, kTcWarps * 32, smem, s>>>(a);
+  CUtensorMap map;
+  std::memset(&map, 0, sizeof(map));
+  a.use_tma = (!kAMN && encode_a_map(a, members, &map)) ? 1 : 0;
+  tc_layer_kernel<EPI, kBK, kAMN><<<grid, kTcWarps * 32, smem, s>>>(a, map);
   return cudaGetLastError();
 }
 
