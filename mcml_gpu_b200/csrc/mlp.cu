@@ -239,6 +239,7 @@ struct TcArgs {
   int splits;               // K split over gridDim.z (member = z / splits, slice = z % splits)
   long long sliceA, sliceW; // element offsets of one K slice in A and W
   int use_tma;              // A chunks by TMA, 128-byte swizzled (K-major A, K % 64 == 0)
+  int use_tma_h;            // H written by TMA from per-warp staging (64-byte swizzle)
 };
 
 __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
@@ -299,7 +300,8 @@ __device__ __forceinline__ void tmem_ld32(uint32_t (&v)[32], uint32_t taddr) {
 // columns are real (N even multiple of 32 means no padding here).
 template <int EPI>
 __device__ __forceinline__ void epilogue32(const TcArgs &g, const uint32_t (&v)[32], int z, int row,
-                                           int c0, const float *bias) {
+                                           int c0, const float *bias, unsigned char *stage,
+                                           int lane) {
   if (EPI == kTcBiasGelu) {
     float *zrow = g.Z ? g.Z + z * g.strideZ + (long long)row * g.ldz + c0 : nullptr;
     uint4 *hrow = reinterpret_cast<uint4 *>(g.H + z * g.strideH + (long long)row * g.ldh + c0);
@@ -315,7 +317,11 @@ __device__ __forceinline__ void epilogue32(const TcArgs &g, const uint32_t (&v)[
       __align__(16) __nv_bfloat162 h[4];
 #pragma unroll
       for (int i = 0; i < 4; ++i) h[i] = __floats2bfloat162_rn(gelu(f[2 * i]), gelu(f[2 * i + 1]));
-      hrow[b] = *reinterpret_cast<const uint4 *>(h);
+      if (stage)  // this lane's row of the warp's 32 x 32 tile, 64-byte swizzled
+        *reinterpret_cast<uint4 *>(stage + lane * 64 + ((b ^ ((lane >> 1) & 3)) * 16)) =
+            *reinterpret_cast<const uint4 *>(h);
+      else
+        hrow[b] = *reinterpret_cast<const uint4 *>(h);
     }
   } else if (EPI == kTcGeluBack) {
     const float4 *zrow =
@@ -330,7 +336,11 @@ __device__ __forceinline__ void epilogue32(const TcArgs &g, const uint32_t (&v)[
       for (int i = 0; i < 4; ++i)
         h[i] = __floats2bfloat162_rn(__uint_as_float(v[b * 8 + 2 * i]) * gelu_grad(zp[2 * i]),
                                      __uint_as_float(v[b * 8 + 2 * i + 1]) * gelu_grad(zp[2 * i + 1]));
-      hrow[b] = *reinterpret_cast<const uint4 *>(h);
+      if (stage)
+        *reinterpret_cast<uint4 *>(stage + lane * 64 + ((b ^ ((lane >> 1) & 3)) * 16)) =
+            *reinterpret_cast<const uint4 *>(h);
+      else
+        hrow[b] = *reinterpret_cast<const uint4 *>(h);
     }
   } else if (EPI == kTcAddF32) {
     float *y = g.Z + z * g.strideZ + (long long)row * g.ldz;
@@ -371,7 +381,8 @@ constexpr int kProducers = 96;  // warps 0-2
 
 template <int EPI, bool kBK, bool kAMN>
 __global__ void __launch_bounds__(kTcWarps * 32, 1)
-    tc_layer_kernel(const TcArgs g, const __grid_constant__ CUtensorMap tmA) {
+    tc_layer_kernel(const TcArgs g, const __grid_constant__ CUtensorMap tmA,
+                    const __grid_constant__ CUtensorMap tmH) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   // 1024-byte aligned base (the swizzled A tiles need it)
   unsigned char *smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
@@ -389,7 +400,10 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1)
   const bool tma = g.use_tma != 0;
   unsigned char *sB = smem;
   unsigned char *sA = smem + (((size_t)K * N * 2 + 1023) & ~(size_t)1023);
-  float *sBias = reinterpret_cast<float *>(sA + (size_t)nslots * slot_bytes);
+  // per epilogue warp two 2 KB staging tiles for the TMA stores of H
+  unsigned char *sStage = sA + (size_t)nslots * slot_bytes;
+  const size_t stage_bytes = g.use_tma_h ? (size_t)8 * 2 * 2048 : 0;
+  float *sBias = reinterpret_cast<float *>(sStage + stage_bytes);
   uint64_t *bars = reinterpret_cast<uint64_t *>(sBias + 256);
   uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 36);
   const uint32_t sA_u = smem_u32(sA), sB_u = smem_u32(sB), bars_u = smem_u32(bars);
@@ -603,16 +617,40 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1)
       const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * N);
       if ((N / 2) % 32 == 0) {
         const int chunks = (N / 2) / 32;
+        unsigned char *my_stage = g.use_tma_h ? sStage + (warp - 4) * 4096 : nullptr;
+        const int row0 = tile * TCM + q * 32;
+        // one 32-column chunk: bias/GELU in registers, then either direct
+        // stores or this warp's staging tile handed to a TMA store
+        auto emit = [&](const uint32_t (&v)[32], int c0, int buf) {
+          unsigned char *st = my_stage ? my_stage + buf * 2048 : nullptr;
+          if (st) {
+            if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 1;\n" ::: "memory");
+            __syncwarp();
+          }
+          if (row < g.M) epilogue32<EPI>(g, v, z, row, c0, sBias, st, lane);
+          if (st) {
+            asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+            __syncwarp();
+            if (lane == 0) {
+              asm volatile(
+                  "cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%2, %3, %4}], [%1];\n" ::"l"(
+                      reinterpret_cast<uint64_t>(&tmH)),
+                  "r"(smem_u32(st)), "r"(c0), "r"(row0), "r"(z)
+                  : "memory");
+              asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+            }
+          }
+        };
         uint32_t va[32], vb[32];
         tmem_ld32(va, tbase + c_begin);
         tmem_wait();
         for (int c = 0; c < chunks; c += 2) {
           if (c + 1 < chunks) tmem_ld32(vb, tbase + c_begin + (c + 1) * 32);
-          if (row < g.M) epilogue32<EPI>(g, va, z, row, c_begin + c * 32, sBias);
+          emit(va, c_begin + c * 32, 0);
           tmem_wait();
           if (c + 1 < chunks) {
             if (c + 2 < chunks) tmem_ld32(va, tbase + c_begin + (c + 2) * 32);
-            if (row < g.M) epilogue32<EPI>(g, vb, z, row, c_begin + (c + 1) * 32, sBias);
+            emit(vb, c_begin + (c + 1) * 32, 1);
             tmem_wait();
           }
         }
@@ -665,6 +703,8 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1)
     }
   }
   asm volatile("cp.async.wait_all;\n" ::: "memory");
+  if (g.use_tma_h && warp >= 4 && lane == 0)
+    asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");  // H stores done
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   __syncthreads();
   if (warp == 0) {
@@ -682,18 +722,21 @@ size_t tc_slot_bytes(int K) { return (size_t)(K < 64 ? K : 64) / 8 * kLboA; }
 // A ring slots: as many as fit beside the weights (at most 16).
 size_t tc_align1k(size_t n) { return (n + 1023) & ~(size_t)1023; }
 
-// A ring slots: as many as fit beside the weights (at most 16).
-int tc_slots(int K, int N) {
-  const size_t room = kTcSmemMax - tc_align1k((size_t)K * N * 2) - kTcSmemFixed - 1024;
+constexpr size_t kTcStageBytes = 8 * 2 * 2048;  // H staging for TMA stores
+
+// A ring slots: as many as fit beside the weights and the staging (at most 16).
+int tc_slots(int K, int N, bool stage) {
+  const size_t room = kTcSmemMax - tc_align1k((size_t)K * N * 2) - kTcSmemFixed - 1024 -
+                      (stage ? kTcStageBytes : 0);
   return (int)std::min<size_t>(16, room / tc_slot_bytes(K));
 }
 
-size_t tc_smem_bytes(int K, int N, int slots) {
+size_t tc_smem_bytes(int K, int N, int slots, bool stage) {
   // weights, A ring, bias + barriers, 1 KB of alignment slack; at least
   // 120 KB so that one CTA runs per SM and its tensor-memory allocation
   // never waits for another's
   const size_t need = tc_align1k((size_t)K * N * 2) + (size_t)slots * tc_slot_bytes(K) +
-                      kTcSmemFixed + 1024;
+                      kTcSmemFixed + 1024 + (stage ? kTcStageBytes : 0);
   return std::max<size_t>(need, 120 * 1024);
 }
 
@@ -737,14 +780,34 @@ bool encode_a_map(const TcArgs &g, int members, CUtensorMap *map) {
             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// Tensor map of H as (column, row, member) for 32 x 32 store boxes with
+// 64-byte swizzling, matching the epilogue warps' staging tiles.
+bool encode_h_map(const TcArgs &g, int members, CUtensorMap *map) {
+  EncodeTiledFn fn = encode_tiled();
+  if (!fn || !g.H) return false;
+  const cuuint64_t dims[3] = {(cuuint64_t)g.N, (cuuint64_t)g.M, (cuuint64_t)members};
+  const cuuint64_t strides[2] = {(cuuint64_t)g.ldh * 2, (cuuint64_t)g.strideH * 2};
+  const cuuint32_t box[3] = {32, 32, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  if (strides[0] % 16 || (members > 1 && strides[1] % 16) || ((uintptr_t)g.H & 15)) return false;
+  return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, g.H, dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <int EPI, bool kBK = false, bool kAMN = false>
 cudaError_t tc_layer(const TcArgs &g, int members, cudaStream_t s) {
   if (g.N % 16 || g.N < 16 || g.N > 256 || g.K % 16 || g.K < 16 || g.K > 256 || g.n_valid > g.N)
     return cudaErrorInvalidValue;
   TcArgs a = g;
-  a.slots = tc_slots(g.K, g.N);
+  CUtensorMap hmap;
+  std::memset(&hmap, 0, sizeof(hmap));
+  const bool stage = (EPI == kTcBiasGelu || EPI == kTcGeluBack) && (g.N / 2) % 32 == 0 &&
+                     g.n_valid == g.N && encode_h_map(g, members, &hmap);
+  a.use_tma_h = stage ? 1 : 0;
+  a.slots = tc_slots(g.K, g.N, stage);
   if (a.slots < 2) return cudaErrorInvalidValue;
-  const size_t smem = tc_smem_bytes(g.K, g.N, a.slots);
+  const size_t smem = tc_smem_bytes(g.K, g.N, a.slots, stage);
   static bool configured[64] = {};  // per device: the attribute is per context
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -770,7 +833,7 @@ cudaError_t tc_layer(const TcArgs &g, int members, cudaStream_t s) {
   CUtensorMap map;
   std::memset(&map, 0, sizeof(map));
   a.use_tma = (!kAMN && encode_a_map(a, members, &map)) ? 1 : 0;
-  tc_layer_kernel<EPI, kBK, kAMN><<<grid, kTcWarps * 32, smem, s>>>(a, map);
+  tc_layer_kernel<EPI, kBK, kAMN><<<grid, kTcWarps * 32, smem, s>>>(a, map, hmap);
   return cudaGetLastError();
 }
 
