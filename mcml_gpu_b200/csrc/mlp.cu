@@ -1021,7 +1021,9 @@ int ensure_cap(mcml_mlp *p, int rows) {
 // Forward of all members on rows [0, n) already gathered into d_x, on the
 // tensor cores (tc_layer_kernel): hidden layers keep Z (FP32) for the
 // backward pass and H (BF16) for the next layer; the output layer writes Y.
-int forward(mcml_mlp *p, int n, bool keep_z) {
+// shared_x: every member reads the same normalised input rows (inference),
+// gathered once instead of once per member.
+int forward(mcml_mlp *p, int n, bool keep_z, bool shared_x = false) {
   const long long H = p->hidden, cap = p->cap, P = p->stride, D = p->depth;
   for (int l = 0; l < p->layers; ++l) {
     TcArgs g;
@@ -1033,7 +1035,7 @@ int forward(mcml_mlp *p, int n, bool keep_z) {
     if (l == 0) {
       g.A = p->d_x;
       g.lda = p->in_pad;
-      g.strideA = cap * p->in_pad;
+      g.strideA = shared_x ? 0 : cap * p->in_pad;
     } else {
       g.A = p->d_h + (long long)(l - 1) * cap * H;
       g.lda = H;
@@ -1451,11 +1453,11 @@ int mcml_mlp_predict(mcml_mlp *p, const float *X, uint64_t n, float *mean, float
   const long long cap = p->cap;
   for (uint64_t r0 = 0; r0 < n; r0 += cap) {
     const int rows = (int)std::min<uint64_t>(cap, n - r0);
-    gather_x_kernel<<<dim3((unsigned)((rows * p->in_pad + 255) / 256), 1, p->E), 256, 0, p->stream>>>(
+    gather_x_kernel<<<dim3((unsigned)((rows * p->in_pad + 255) / 256), 1, 1), 256, 0, p->stream>>>(
         X + r0 * p->in_dim, nullptr, rows, p->in_dim, p->in_pad, p->d_xmean, p->d_xinv, 0, p->d_x,
         cap * p->in_pad);
     MLP_TRY(cudaGetLastError());
-    rc = forward(p, rows, false);
+    rc = forward(p, rows, false, true);
     if (rc) return rc;
     ensemble_kernel<<<(unsigned)(((long long)rows * p->out_dim + 255) / 256), 256, 0, p->stream>>>(
         p->d_y, cap * p->out_dim, p->E, (long long)rows * p->out_dim, p->d_tmean, p->d_tstd,
