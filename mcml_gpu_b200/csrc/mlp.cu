@@ -28,9 +28,11 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <random>
 #include <string>
 #include <vector>
@@ -749,9 +751,8 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t
 // link-time dependency on the driver library); null if unavailable.
 EncodeTiledFn encode_tiled() {
   static EncodeTiledFn fn = nullptr;
-  static bool tried = false;
-  if (!tried) {
-    tried = true;
+  static std::once_flag once;
+  std::call_once(once, [] {
     void *ptr = nullptr;
     cudaDriverEntryPointQueryResult q;
     if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) ==
@@ -760,7 +761,7 @@ EncodeTiledFn encode_tiled() {
       fn = reinterpret_cast<EncodeTiledFn>(ptr);
     else
       cudaGetLastError();
-  }
+  });
   return fn;
 }
 
@@ -808,27 +809,31 @@ cudaError_t tc_layer(const TcArgs &g, int members, cudaStream_t s) {
   a.slots = tc_slots(g.K, g.N, stage);
   if (a.slots < 2) return cudaErrorInvalidValue;
   const size_t smem = tc_smem_bytes(g.K, g.N, a.slots, stage);
-  static bool configured[64] = {};  // per device: the attribute is per context
+  // per device (the attribute belongs to the context); setting it twice
+  // from two threads is harmless, the flags only save the calls
+  static std::atomic<bool> configured[64];
+  static std::atomic<int> sm_count[64];
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-  if (!configured[dev]) {
+  if (!configured[dev].load()) {
     e = cudaFuncSetAttribute(tc_layer_kernel<EPI, kBK, kAMN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)kTcSmemMax);
     if (e != cudaSuccess) return e;
-    configured[dev] = true;
+    configured[dev].store(true);
   }
-  static int sms[64] = {};
-  if (!sms[dev]) {
-    e = cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev);
+  int sms = sm_count[dev].load();
+  if (!sms) {
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
+    sm_count[dev].store(sms);
   }
   // persistent: one CTA per SM shared out among the members, each CTA
   // walking its member's 128-row tiles with the weights resident
   const int tiles = (g.M + TCM - 1) / TCM;
   const int zs = std::max(1, members) * std::max(1, g.splits);
-  const int per_z = std::max(1, sms[dev] / zs);
+  const int per_z = std::max(1, sms / zs);
   dim3 grid(std::min(tiles, per_z), 1, zs);
   CUtensorMap map;
   std::memset(&map, 0, sizeof(map));
