@@ -51,18 +51,26 @@ WORKLOAD = "plain MC + replay, 5-layer tissue, 1e8 photons, -R -A -B"
 #        renormalise 6, 1 cmp                                    44 lane;
 #        rcp x3, rsq x2 (sqrt), sin, cos, rsq                     8 MUFU
 #   survive: 2 cmp                                                2 lane
-# = 98 FP32/INT32 lane ops and 9 MUFU ops.  A B200 SM issues 128
-# thread-instructions per clock (4 schedulers x 32 lanes) and 16 MUFU
-# results, so steps/s <= f_sm * 148 * min(128 / (98 + 9), 16 / 9): the
+# = 98 FP32/INT32 lane ops and 9 MUFU ops.  7 pairs of those lane ops (the
+# x/y halves of the move, of the rotation's five products and sums and of
+# the renormalisation) go out as one sm_100 paired FP32 instruction each
+# (FFMA2/FMUL2), so a step needs 98 - 7 + 9 = 100 issue slots.  A B200 SM
+# issues 128 thread-instructions per clock (4 schedulers x 32 lanes) and 16
+# MUFU results, so steps/s <= f_sm * 148 * min(128 / 100, 16 / 9): the
 # issue rate binds.  ncu's pipe counters agree that MUFU is not the limit:
 # 9.5 XU thread-instructions per step, 91 % of issue slots used.
 OPS_LANE = 98
+OPS_PAIRED = 7
 OPS_MUFU = 9
 SM_COUNT = 148
 
 
+def issue_slots_per_step() -> int:
+    return OPS_LANE - OPS_PAIRED + OPS_MUFU
+
+
 def steps_per_clock_per_sm() -> float:
-    return min(128.0 / (OPS_LANE + OPS_MUFU), 16.0 / OPS_MUFU)
+    return min(128.0 / issue_slots_per_step(), 16.0 / OPS_MUFU)
 
 
 class ClockSampler:
@@ -648,10 +656,11 @@ def mcml_arm(args) -> int:
                      "unit": "Gstep/s", "frac": achieved / peak,
                      "traffic": read_traffic(int(res.slots)),
                      "kernel": "walk_kernel",
-                     "model": f"steps/s <= f_sm x {info.sm_count} SMs x min(128/({OPS_LANE}+"
-                              f"{OPS_MUFU}), 16/{OPS_MUFU}) at the measured median SM clock "
-                              f"(issue bound: 128 thread-instructions/clk/SM); ops counted "
-                              f"by hand per common step",
+                     "model": f"steps/s <= f_sm x {info.sm_count} SMs x min(128/({OPS_LANE}-"
+                              f"{OPS_PAIRED}+{OPS_MUFU}), 16/{OPS_MUFU}) at the measured median "
+                              f"SM clock (issue bound: 128 thread-instructions/clk/SM; "
+                              f"{OPS_PAIRED} lane-op pairs issued as paired FP32 instructions); "
+                              f"ops counted by hand per common step",
                      "walk_ms": walk_kernel_ms, "seed_ms": float(res.seed_ms),
                      "replay_ms": float(rep.replay_ms)},
         "clocks": clocks,

@@ -212,8 +212,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
     }
 
     if (s > 0.0f) {
-      drop_weight_walk(p, L.w, L.z);
-      spin(p, t.lay2[p.layer].x, &st);
+      drop_weight_walk(p, L.w);
+      spin(p, t.hg[p.layer], &st);
     }
 
     if (!survive<true>(p, &st)) {
@@ -330,7 +330,7 @@ __global__ void __launch_bounds__(kBlock) replay_kernel(const __grid_constant__ 
 
       if (s > 0.0f) {
         const float4 L = t.lay[p.layer];
-        const unsigned w_temp = drop_weight(p, L.w, L.z);
+        const unsigned w_temp = drop_weight(p, L.w);
         s_ni[p.layer - 1][tid] += 1u;
         // Absorbance tallies, transport.cu:580-600.
         int iz;
@@ -356,7 +356,7 @@ __global__ void __launch_bounds__(kBlock) replay_kernel(const __grid_constant__ 
             w_run = w_temp;
           }
         }
-        spin(p, t.lay2[p.layer].x, &st);
+        spin(p, t.hg[p.layer], &st);
       }
 
       if (!survive<false>(p, &st)) break;

@@ -160,8 +160,8 @@ __global__ void __launch_bounds__(128) noalloc_walk_kernel(const __grid_constant
     }
     if (s > 0.0f) {
       const float4 L = t.lay[p.layer];
-      drop_weight_walk(p, L.w, L.z);
-      spin(p, t.lay2[p.layer].x, &st);
+      drop_weight_walk(p, L.w);
+      spin(p, t.hg[p.layer], &st);
     }
     if (!survive<true>(p, &st)) {
       steps_acc += (uint32_t)p.steps;
