@@ -22,8 +22,9 @@
 // contraction, one exp2 (MUFU) and one add.  The exponents reach hundreds,
 // so the contraction stays in FP32 on the CUDA cores (a bf16/tf32 tensor
 // product would lose the exponent's low bits).  Photon features are staged
-// through shared memory in chunks and each thread carries kPer combos;
-// the photons are split over blockIdx.y and the partial sums added in FP64.
+// through shared memory in chunks and each thread carries kPer combos over
+// photon pairs on paired FP32 instructions; the photons are split over
+// blockIdx.y and the partial sums added in FP64.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -37,8 +38,8 @@ namespace mcml {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kPer = 4;      // combos per thread
-constexpr int kChunk = 256;  // photons per shared-memory chunk
+constexpr int kPer = 2;      // combos per thread
+constexpr int kChunk = 256;  // photons per shared-memory chunk (even)
 constexpr int kMaxK = 2 * MCML_MAX_LAYERS + 2;
 
 // Packs F_i (k-major within a photon, padded to kMaxK) for every photon.
@@ -57,17 +58,37 @@ __global__ void wmc_pack_kernel(const float *pl, const float *inter, const float
   for (int k = 2 * L + 2; k < kMaxK; ++k) f[k] = 0.0f;
 }
 
+// 2^x on the MUFU unit (PTX ex2.approx, relative error about 2^-22;
+// results below 2^-126 flush to zero, terms far below the photon weights
+// that matter).
+__device__ __forceinline__ float ex2(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// Each thread carries kPer combos and walks the photons two at a time:
+// the pair's features sit interleaved in shared memory, {F_jk, F_j+1,k},
+// so that one 16-byte load feeds two k and every contraction step is one
+// paired FMA (__ffma2_rn) over the two photons against the combo's
+// coefficient held twice in a register pair.  Per term that is K/2
+// paired FMAs, one MUFU exp2, half a paired add and K/(4*kPer) shared
+// loads; the FP32 lanes (K+1 operations per term) are the binding unit.
 template <int K>
 __global__ void __launch_bounds__(kThreads) wmc_kernel(const float *F, uint64_t D,
                                                        const float *coef, uint64_t C,
                                                        double inv_scale, double *out) {
-  __shared__ float sF[kChunk][K];
+  static_assert(K % 2 == 0, "K = 2L+2 is even");
+  __shared__ __align__(16) float2 sF[kChunk / 2][K];  // [photon pair][k]
   const uint64_t c0 = ((uint64_t)blockIdx.x * kThreads + threadIdx.x) * kPer;
-  float a[kPer][K];
+  float2 a[kPer][K];
 #pragma unroll
   for (int r = 0; r < kPer; ++r)
 #pragma unroll
-    for (int k = 0; k < K; ++k) a[r][k] = (c0 + r < C) ? coef[(c0 + r) * kMaxK + k] : 0.0f;
+    for (int k = 0; k < K; ++k) {
+      const float v = (c0 + r < C) ? coef[(c0 + r) * kMaxK + k] : 0.0f;
+      a[r][k] = make_float2(v, v);
+    }
   double total[kPer];
 #pragma unroll
   for (int r = 0; r < kPer; ++r) total[r] = 0.0;
@@ -79,30 +100,40 @@ __global__ void __launch_bounds__(kThreads) wmc_kernel(const float *F, uint64_t 
   const uint64_t d1 = d0 + per * kChunk < D ? d0 + per * kChunk : D;
   for (uint64_t base = d0; base < d1; base += kChunk) {
     const int n = (int)((d1 - base) < (uint64_t)kChunk ? (d1 - base) : (uint64_t)kChunk);
+    const int np = (n + 1) / 2;
     __syncthreads();
-    for (int idx = threadIdx.x; idx < n * K; idx += kThreads) {
-      const int j = idx / K, k = idx % K;
-      sF[j][k] = F[(base + j) * kMaxK + k];
+    for (int idx = threadIdx.x; idx < np * K; idx += kThreads) {
+      const int jp = idx / K, k = idx % K;
+      const int j = 2 * jp;
+      const float f0 = F[(base + j) * kMaxK + k];
+      // a missing partner (odd n) is a photon of weight 0: log2 w = -inf
+      // (k = K-2) and 0 elsewhere, so its exp2 term is exactly 0
+      const float f1 = j + 1 < n ? F[(base + j + 1) * kMaxK + k] : (k == K - 2 ? -INFINITY : 0.0f);
+      sF[jp][k] = make_float2(f0, f1);
     }
     __syncthreads();
-    float acc[kPer];
+    float2 acc[kPer];
 #pragma unroll
-    for (int r = 0; r < kPer; ++r) acc[r] = 0.0f;
-    for (int j = 0; j < n; ++j) {
-      float e[kPer];
+    for (int r = 0; r < kPer; ++r) acc[r] = make_float2(0.0f, 0.0f);
+    for (int jp = 0; jp < np; ++jp) {
+      float2 e[kPer];
 #pragma unroll
-      for (int r = 0; r < kPer; ++r) e[r] = 0.0f;
+      for (int r = 0; r < kPer; ++r) e[r] = make_float2(0.0f, 0.0f);
 #pragma unroll
-      for (int k = 0; k < K; ++k) {
-        const float f = sF[j][k];
+      for (int k = 0; k < K; k += 2) {
+        const float4 f = *reinterpret_cast<const float4 *>(&sF[jp][k]);
 #pragma unroll
-        for (int r = 0; r < kPer; ++r) e[r] = fmaf(a[r][k], f, e[r]);
+        for (int r = 0; r < kPer; ++r) e[r] = __ffma2_rn(a[r][k], make_float2(f.x, f.y), e[r]);
+#pragma unroll
+        for (int r = 0; r < kPer; ++r)
+          e[r] = __ffma2_rn(a[r][k + 1], make_float2(f.z, f.w), e[r]);
       }
 #pragma unroll
-      for (int r = 0; r < kPer; ++r) acc[r] += exp2f(e[r]);
+      for (int r = 0; r < kPer; ++r)
+        acc[r] = __fadd2_rn(acc[r], make_float2(ex2(e[r].x), ex2(e[r].y)));
     }
 #pragma unroll
-    for (int r = 0; r < kPer; ++r) total[r] += (double)acc[r];
+    for (int r = 0; r < kPer; ++r) total[r] += (double)acc[r].x + (double)acc[r].y;
   }
 #pragma unroll
   for (int r = 0; r < kPer; ++r)
