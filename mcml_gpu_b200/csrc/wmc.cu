@@ -39,7 +39,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kPer = 2;      // combos per thread
-constexpr int kChunk = 256;  // photons per shared-memory chunk (even)
+constexpr int kChunk = 256;  // photons per shared-memory chunk (a multiple of 4)
 constexpr int kMaxK = 2 * MCML_MAX_LAYERS + 2;
 
 // Packs F_i (k-major within a photon, padded to kMaxK) for every photon.
@@ -67,15 +67,16 @@ __device__ __forceinline__ float ex2(float x) {
   return y;
 }
 
-// Each thread carries kPer combos and walks the photons two at a time:
-// the pair's features sit interleaved in shared memory, {F_jk, F_j+1,k},
-// so that one 16-byte load feeds two k and every contraction step is one
-// paired FMA (__ffma2_rn) over the two photons against the combo's
-// coefficient held twice in a register pair.  Per term that is K/2
+// Each thread carries kPer combos and walks the photons in pairs: a pair's
+// features sit interleaved in shared memory, {F_jk, F_j+1,k}, so that one
+// 16-byte load feeds two k and every contraction step is one paired FMA
+// (__ffma2_rn) over the two photons against the combo's coefficient held
+// twice in a register pair.  Two pairs are taken per iteration, which
+// gives each thread 2*kPer independent FMA chains.  Per term that is K/2
 // paired FMAs, one MUFU exp2, half a paired add and K/(4*kPer) shared
 // loads; the FP32 lanes (K+1 operations per term) are the binding unit.
 template <int K>
-__global__ void __launch_bounds__(kThreads) wmc_kernel(const float *F, uint64_t D,
+__global__ void __launch_bounds__(kThreads, 4) wmc_kernel(const float *F, uint64_t D,
                                                        const float *coef, uint64_t C,
                                                        double inv_scale, double *out) {
   static_assert(K % 2 == 0, "K = 2L+2 is even");
@@ -100,37 +101,46 @@ __global__ void __launch_bounds__(kThreads) wmc_kernel(const float *F, uint64_t 
   const uint64_t d1 = d0 + per * kChunk < D ? d0 + per * kChunk : D;
   for (uint64_t base = d0; base < d1; base += kChunk) {
     const int n = (int)((d1 - base) < (uint64_t)kChunk ? (d1 - base) : (uint64_t)kChunk);
-    const int np = (n + 1) / 2;
+    const int np = (n + 3) / 4 * 2;  // photon pairs, an even number (padding below)
     __syncthreads();
     for (int idx = threadIdx.x; idx < np * K; idx += kThreads) {
       const int jp = idx / K, k = idx % K;
       const int j = 2 * jp;
-      const float f0 = F[(base + j) * kMaxK + k];
-      // a missing partner (odd n) is a photon of weight 0: log2 w = -inf
-      // (k = K-2) and 0 elsewhere, so its exp2 term is exactly 0
-      const float f1 = j + 1 < n ? F[(base + j + 1) * kMaxK + k] : (k == K - 2 ? -INFINITY : 0.0f);
+      // photons past n (padding to whole pairs of pairs) have weight 0:
+      // log2 w = -inf (k = K-2) and 0 elsewhere, so their exp2 term is 0
+      const float pad = k == K - 2 ? -INFINITY : 0.0f;
+      const float f0 = j < n ? F[(base + j) * kMaxK + k] : pad;
+      const float f1 = j + 1 < n ? F[(base + j + 1) * kMaxK + k] : pad;
       sF[jp][k] = make_float2(f0, f1);
     }
     __syncthreads();
     float2 acc[kPer];
 #pragma unroll
     for (int r = 0; r < kPer; ++r) acc[r] = make_float2(0.0f, 0.0f);
-    for (int jp = 0; jp < np; ++jp) {
-      float2 e[kPer];
+    for (int jp = 0; jp < np; jp += 2) {  // pairs jp and jp+1, added in order
+      float2 e[2][kPer];
 #pragma unroll
-      for (int r = 0; r < kPer; ++r) e[r] = make_float2(0.0f, 0.0f);
+      for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int r = 0; r < kPer; ++r) e[h][r] = make_float2(0.0f, 0.0f);
 #pragma unroll
       for (int k = 0; k < K; k += 2) {
-        const float4 f = *reinterpret_cast<const float4 *>(&sF[jp][k]);
 #pragma unroll
-        for (int r = 0; r < kPer; ++r) e[r] = __ffma2_rn(a[r][k], make_float2(f.x, f.y), e[r]);
+        for (int h = 0; h < 2; ++h) {
+          const float4 f = *reinterpret_cast<const float4 *>(&sF[jp + h][k]);
 #pragma unroll
-        for (int r = 0; r < kPer; ++r)
-          e[r] = __ffma2_rn(a[r][k + 1], make_float2(f.z, f.w), e[r]);
+          for (int r = 0; r < kPer; ++r)
+            e[h][r] = __ffma2_rn(a[r][k], make_float2(f.x, f.y), e[h][r]);
+#pragma unroll
+          for (int r = 0; r < kPer; ++r)
+            e[h][r] = __ffma2_rn(a[r][k + 1], make_float2(f.z, f.w), e[h][r]);
+        }
       }
 #pragma unroll
-      for (int r = 0; r < kPer; ++r)
-        acc[r] = __fadd2_rn(acc[r], make_float2(ex2(e[r].x), ex2(e[r].y)));
+      for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int r = 0; r < kPer; ++r)
+          acc[r] = __fadd2_rn(acc[r], make_float2(ex2(e[h][r].x), ex2(e[h][r].y)));
     }
 #pragma unroll
     for (int r = 0; r < kPer; ++r) total[r] += (double)acc[r].x + (double)acc[r].y;
