@@ -149,37 +149,44 @@ int build_params(mcml_ctx *c) {
   return MCML_OK;
 }
 
+// Checks the simulation and sizes the slot states before anything of the
+// context changes: a rejected simulation leaves the previous one in place,
+// and a failed allocation leaves no simulation that launch_run accepts.
 int set_sim(mcml_ctx *c, const mcml_sim *sim) {
-  int rc = derive(sim, &c->der);
+  mcml_derived der{};
+  int rc = derive(sim, &der);
   if (rc) return rc;
-  c->sim = *sim;
-  c->N = sim->number_photons;
+  const uint64_t N = sim->number_photons;
   const uint64_t ref_threads = (uint64_t)c->sm_count * (uint64_t)c->max_thr_sm;
   uint64_t S;
   if (c->opts.slots) {
     S = c->opts.slots;
-  } else if (c->N <= ref_threads) {
-    S = c->N;  // the reference's layout: photon t is thread t's first photon
+  } else if (N <= ref_threads) {
+    S = N;  // the reference's layout: photon t is thread t's first photon
   } else {
-    S = (c->N + kPhotonsPerSlot - 1) / kPhotonsPerSlot;
+    S = (N + kPhotonsPerSlot - 1) / kPhotonsPerSlot;
     S = std::max(S, ref_threads);
     S = std::min(S, std::max(kMaxAutoSlots, ref_threads));
   }
-  if (S > c->N) S = c->N;
-  if (c->N / S >= 0xFFFFFFFFull)
+  if (S > N) S = N;
+  if (N / S >= 0xFFFFFFFFull)
     return set_error(MCML_E_INVALID, "too many photons per slot; raise mcml_opts.slots");
   if (S >= 0xFFFFFFFFull) return set_error(MCML_E_INVALID, "slots must be below 2^32");
-  if (c->N >= (1ull << 44)) return set_error(MCML_E_INVALID, "number_photons must be below 2^44");
-  c->S = S;
+  if (N >= (1ull << 44)) return set_error(MCML_E_INVALID, "number_photons must be below 2^44");
   const uint64_t nz = grid_nz(c), nr = grid_nr(c);
   if (nr == 0 || nz == 0 || (uint64_t)sim->num_sds * nz * nr >= (1ull << 31))
     return set_error(MCML_E_INVALID, "absorbance grid too large");
   DeviceGuard g(c->device);
   if (S > c->slot_cap) {
     dfree(c->d_slot_state);
+    c->slot_cap = 0;
     CUDA_TRY(cudaMalloc(&c->d_slot_state, S * 3 * sizeof(uint2)));
     c->slot_cap = S;
   }
+  c->der = der;
+  c->sim = *sim;
+  c->N = N;
+  c->S = S;
   build_params(c);
   c->ran = c->replayed = c->host_valid = false;
   return MCML_OK;
@@ -294,6 +301,8 @@ int fetch_host(mcml_ctx *c) {
 }
 
 int launch_run(mcml_ctx *c) {
+  if (!c->d_slot_state || c->S > c->slot_cap)
+    return set_error(MCML_E_STATE, "no simulation set: the last mcml_set_sim failed");
   DeviceGuard g(c->device);
   CUDA_TRY(cudaMemsetAsync(c->d_counters, 0, kCntWords * sizeof(unsigned long long), c->stream));
   CUDA_TRY(cudaMemsetAsync(c->d_sums, 0, 96 * sizeof(unsigned long long), c->stream));
@@ -593,6 +602,8 @@ int mcml_run(mcml_ctx *ctx, mcml_result *result) {
 int mcml_run_checkpointed(mcml_ctx *c, const mcml_checkpoint_opts *ck, mcml_result *result) {
   clear_error();
   if (!c || !ck || !ck->path || !ck->path[0]) return set_error(MCML_E_INVALID, "null argument");
+  if (!c->d_slot_state || c->S > c->slot_cap)
+    return set_error(MCML_E_STATE, "no simulation set: the last mcml_set_sim failed");
   DeviceGuard g(c->device);
   const std::string path = ck->path;
   const uint64_t digest = run_digest(c->sim, c->opts.seed, c->opts.slot_begin, c->S);
