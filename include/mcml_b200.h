@@ -169,7 +169,10 @@ int mcml_derive(const mcml_sim *sim, mcml_derived *out);
 /* ---- simulation ------------------------------------------------------- */
 /* Replaces InitMemStructs + InitDCMem (transport.cu:1002-1070). */
 int mcml_create(const mcml_sim *sim, const mcml_opts *opts, mcml_ctx **ctx);
-/* Uploads a new parameter block to an existing context (same limits). */
+/* Uploads a new parameter block to an existing context (same limits).  A
+ * simulation rejected as invalid leaves the previous one in place; if the
+ * slot states cannot be allocated (MCML_E_CUDA), runs return MCML_E_STATE
+ * until a later mcml_set_sim succeeds. */
 int mcml_set_sim(mcml_ctx *ctx, const mcml_sim *sim);
 void mcml_destroy(mcml_ctx *ctx);
 
