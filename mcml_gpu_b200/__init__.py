@@ -282,6 +282,27 @@ def load_library() -> C.CDLL:
     return lib
 
 
+def _device_ptr(t, name: str, *, device: int, shape: Optional[tuple] = None) -> C.c_void_p:
+    """Address of a torch tensor handed to a kernel: it must be a C-contiguous
+    float32 tensor on CUDA device `device`, of `shape` where given (None
+    entries match any size).  A host tensor's address would be read by the
+    GPU as a device address; a strided or differently typed one would be
+    read as garbage -- both are rejected here instead."""
+    import torch
+    if not isinstance(t, torch.Tensor):
+        raise TypeError(f"{name}: expected a torch tensor, got {type(t).__name__}")
+    if t.device.type != "cuda" or t.device.index != device:
+        raise ValueError(f"{name}: must be on cuda:{device}, is on {t.device}")
+    if t.dtype != torch.float32:
+        raise ValueError(f"{name}: must be float32, is {t.dtype}")
+    if not t.is_contiguous():
+        raise ValueError(f"{name}: must be contiguous")
+    if shape is not None and (t.dim() != len(shape) or
+                              any(w is not None and w != g for w, g in zip(shape, t.shape))):
+        raise ValueError(f"{name}: shape {tuple(t.shape)}, expected {shape}")
+    return C.c_void_p(t.data_ptr())
+
+
 def _check(rc: int, where: str) -> None:
     if rc != 0:
         lib = load_library()

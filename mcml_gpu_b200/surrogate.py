@@ -22,7 +22,7 @@ from typing import Optional, Sequence
 
 import numpy as np
 
-from . import Batch, Simulation, Sim, _check, load_library
+from . import Batch, Simulation, Sim, _check, _device_ptr, load_library
 from . import wmc
 
 __all__ = ["MLP", "features", "make_labels", "Surrogate", "BOUND"]
@@ -66,10 +66,6 @@ def _bind(lib):
     lib._mlp_bound = True
 
 
-def _ptr(t):
-    return C.c_void_p(t.data_ptr())
-
-
 class MLP:
     """Ensemble of MLPs (in -> hidden x depth, GELU -> out) on the GPU."""
 
@@ -111,17 +107,26 @@ class MLP:
     def gradients(self, X, T):
         """X: (n, in) and T: (n, out) float32 CUDA tensors -> (loss[E], grads[E, P])."""
         n = X.shape[0]
+        px, pt = self._xt(X, T)
         loss = np.empty(self.ensemble, np.float32)
         grads = np.empty((self.ensemble, self.num_params), np.float32)
-        _check(self.lib.mcml_mlp_gradients(self._h, _ptr(X), _ptr(T), n,
+        _check(self.lib.mcml_mlp_gradients(self._h, px, pt, n,
                                            loss.ctypes.data_as(C.c_void_p),
                                            grads.ctypes.data_as(C.c_void_p)),
                "mcml_mlp_gradients")
         return loss, grads
 
+    def _xt(self, X, T):
+        """Checked device addresses of inputs X (n, in) and targets T (n, out)."""
+        n = X.shape[0] if hasattr(X, "shape") else None
+        return (_device_ptr(X, "X", device=self.device, shape=(None, self.in_dim)),
+                _device_ptr(T, "T", device=self.device, shape=(n, self.out_dim)))
+
     def train_epoch(self, X, T, *, batch: int = 4096, lr: float = 1e-3, seed: int = 0):
+        """One epoch over X (n, in) and T (n, out), float32 CUDA tensors."""
+        px, pt = self._xt(X, T)
         loss = np.empty(self.ensemble, np.float32)
-        _check(self.lib.mcml_mlp_train_epoch(self._h, _ptr(X), _ptr(T), X.shape[0], batch, lr,
+        _check(self.lib.mcml_mlp_train_epoch(self._h, px, pt, X.shape[0], batch, lr,
                                              seed, loss.ctypes.data_as(C.c_void_p)),
                "mcml_mlp_train_epoch")
         return loss
@@ -129,10 +134,12 @@ class MLP:
     def predict(self, X, chunk: int = 65536):
         """X: (n, in) float32 CUDA tensor -> (mean, spread) CUDA tensors (n, out)."""
         import torch
+        px = _device_ptr(X, "X", device=self.device, shape=(None, self.in_dim))
         n = X.shape[0]
         mean = torch.empty((n, self.out_dim), dtype=torch.float32, device=X.device)
         spread = torch.empty_like(mean)
-        _check(self.lib.mcml_mlp_predict(self._h, _ptr(X), n, _ptr(mean), _ptr(spread), chunk),
+        _check(self.lib.mcml_mlp_predict(self._h, px, n, C.c_void_p(mean.data_ptr()),
+                                         C.c_void_p(spread.data_ptr()), chunk),
                "mcml_mlp_predict")
         _check(self.lib.mcml_mlp_sync(self._h), "mcml_mlp_sync")
         return mean, spread

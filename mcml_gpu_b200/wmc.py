@@ -11,7 +11,7 @@ import ctypes as C
 
 import numpy as np
 
-from . import MAX_LAYERS, _check, load_library
+from . import MAX_LAYERS, _check, _device_ptr, load_library
 
 __all__ = ["WmcSet", "Prepared", "rescale", "rescale_reference"]
 
@@ -62,6 +62,7 @@ class Prepared:
         lib = load_library()
         _bind(lib)
         dev = torch.device("cuda", self.device)
+        pc = _device_ptr(combos, "combos", device=self.device, shape=(None, 2 * self.L))
         Cn = combos.shape[0]
         out = torch.empty(Cn, dtype=torch.float64, device=dev)
         nbytes = int(lib.mcml_wmc_workspace_bytes(self.D, Cn))
@@ -71,7 +72,7 @@ class Prepared:
         bm = (C.c_float * MAX_LAYERS)(*[float(v) for v in base_mua][:self.L])
         bs = (C.c_float * MAX_LAYERS)(*[float(v) for v in base_mus][:self.L])
         stream = torch.cuda.current_stream(dev).cuda_stream
-        _check(lib.mcml_wmc_rescale(C.byref(s), bm, bs, C.c_void_p(combos.data_ptr()), Cn,
+        _check(lib.mcml_wmc_rescale(C.byref(s), bm, bs, pc, Cn,
                                     float(0xFFFFFFFF) * float(photons), C.c_void_p(out.data_ptr()),
                                     C.c_void_p(self._ws.data_ptr()), self._ws.numel(),
                                     C.c_void_p(stream)),

@@ -219,3 +219,14 @@ def test_row_text_matches_iostream_default_format():
     want = "".join("".join("%g\t" % float(v) for v in r) + "\n" for r in rows).encode()
     assert m.format_rows_text(rows) == want
     assert m.format_rows_text(np.zeros((0, 7), np.float32)) == b""
+
+
+def test_device_tensor_checks_reject_host_memory():
+    """Tensors handed to kernels must be CUDA tensors: a host tensor's
+    address would be read by the GPU as a device address."""
+    import torch
+    from mcml_gpu_b200 import _device_ptr
+    with pytest.raises(TypeError):
+        _device_ptr(np.zeros((4, 25), np.float32), "X", device=0)
+    with pytest.raises(ValueError, match="cuda:0"):
+        _device_ptr(torch.zeros((4, 25)), "X", device=0, shape=(None, 25))

@@ -148,3 +148,22 @@ def test_tensor_core_forward_matches_cpu_reference(hidden, depth, n, gpu_availab
     scale = float(np.abs(ys).mean())
     assert np.max(np.abs(mean.cpu().numpy() - ys.mean(0))) < 1e-2 * scale
     assert np.max(np.abs(spread.cpu().numpy() - ys.std(0))) < 1e-2 * scale
+
+
+@pytest.mark.gpu
+def test_tensor_arguments_are_checked(gpu_available):
+    """Wrongly typed, strided or shaped inputs are rejected before any launch."""
+    mlp = sg.MLP(25, 3, hidden=64, depth=3, ensemble=2, seed=1)
+    dev = torch.device("cuda", 0)
+    X = torch.zeros((64, 25), dtype=torch.float32, device=dev)
+    T = torch.zeros((64, 3), dtype=torch.float32, device=dev)
+    with pytest.raises(ValueError, match="float32"):
+        mlp.predict(X.double())
+    with pytest.raises(ValueError, match="contiguous"):
+        mlp.predict(torch.zeros((25, 64), device=dev).t())
+    with pytest.raises(ValueError, match="shape"):
+        mlp.predict(X[:, :24].contiguous())
+    with pytest.raises(ValueError, match="shape"):
+        mlp.train_epoch(X, T[:32], batch=32)
+    mean, spread = mlp.predict(X)  # the checked path still runs
+    assert mean.shape == (64, 3) and spread.shape == (64, 3)
