@@ -14,7 +14,10 @@
 //                  from it when it exists (<file>.<i> for simulation i > 0)
 //   -batch         every simulation of the file in one batched launch
 //                  (first pass only: output.txt and summary.json)
+#include <cctype>
+#include <cerrno>
 #include <chrono>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <ctime>
@@ -25,6 +28,28 @@
 #include "../../include/mcml_b200.h"
 
 namespace {
+
+// Values of this CLI's own options (-S, -T, -grid): the whole argument
+// must be the number, so a typo is reported instead of read as 0.
+bool parse_u64(const char *s, unsigned long long *out) {
+  if (!s || !std::isdigit((unsigned char)s[0])) return false;
+  errno = 0;
+  char *end = nullptr;
+  const unsigned long long v = std::strtoull(s, &end, 10);
+  if (errno == ERANGE || *end != '\0') return false;
+  *out = v;
+  return true;
+}
+
+bool parse_length(const char *s, float *out) {
+  if (!s || !*s) return false;
+  errno = 0;
+  char *end = nullptr;
+  const float v = std::strtof(s, &end);
+  if (errno == ERANGE || *end != '\0' || !std::isfinite(v) || !(v > 0.0f)) return false;
+  *out = v;
+  return true;
+}
 
 void show_usage(const std::string &name) {
   const size_t found = name.find_last_of("/\\");
@@ -124,18 +149,36 @@ int main(int argc, char *argv[]) {
     } else if (a == "-LS") {
       list_gpus(true);
       return 0;
-    } else if (a == "-S" && i + 1 < argc) {
-      seed = std::strtoull(argv[++i], nullptr, 10);
+    } else if (a == "-S") {
+      if (i + 1 >= argc || !parse_u64(argv[i + 1], &seed)) {
+        std::cout << "-S option needs a seed (an unsigned integer)!\n";
+        return 0;
+      }
+      ++i;
       have_seed = true;
-    } else if (a == "-T" && i + 1 < argc) {
-      slots = std::strtoull(argv[++i], nullptr, 10);
-    } else if (a == "-grid" && i + 4 < argc) {
-      grid_nr = (unsigned)std::strtoul(argv[i + 1], nullptr, 10);
-      grid_nz = (unsigned)std::strtoul(argv[i + 2], nullptr, 10);
-      grid_dr = std::strtof(argv[i + 3], nullptr);
-      grid_dz = std::strtof(argv[i + 4], nullptr);
+    } else if (a == "-T") {
+      if (i + 1 >= argc || !parse_u64(argv[i + 1], &slots)) {
+        std::cout << "-T option needs a slot count (an unsigned integer, 0 for automatic)!\n";
+        return 0;
+      }
+      ++i;
+    } else if (a == "-grid") {
+      unsigned long long nr = 0, nz = 0;
+      if (i + 4 >= argc || !parse_u64(argv[i + 1], &nr) || !parse_u64(argv[i + 2], &nz) ||
+          nr == 0 || nz == 0 || nr > 0x7fffffffull || nz > 0x7fffffffull ||
+          !parse_length(argv[i + 3], &grid_dr) || !parse_length(argv[i + 4], &grid_dz)) {
+        std::cout << "-grid option needs nr nz dr dz (two positive cell counts, two positive "
+                     "cell sizes in cm)!\n";
+        return 0;
+      }
+      grid_nr = (unsigned)nr;
+      grid_nz = (unsigned)nz;
       i += 4;
-    } else if (a == "-CK" && i + 1 < argc) {
+    } else if (a == "-CK") {
+      if (i + 1 >= argc) {
+        std::cout << "-CK option needs a checkpoint file name!\n";
+        return 0;
+      }
       checkpoint = argv[++i];
     } else if (a == "-batch") {
       do_batch = true;

@@ -148,6 +148,26 @@ def test_cli_usage_and_flag_rules():
     assert r.returncode == 0 and "GPU selection ERROR!" in r.stdout
 
 
+@pytest.mark.parametrize("flags,msg", [
+    (["-S", "12ab"], "-S option needs a seed"),
+    (["-S", "-5"], "-S option needs a seed"),
+    (["-S"], "-S option needs a seed"),
+    (["-T", "many"], "-T option needs a slot count"),
+    (["-grid", "200", "200", "0.005"], "-grid option needs nr nz dr dz"),
+    (["-grid", "0", "200", "0.005", "0.005"], "-grid option needs nr nz dr dz"),
+    (["-grid", "200", "200", "-0.005", "0.005"], "-grid option needs nr nz dr dz"),
+    (["-grid", "200", "200", "0.005", "x"], "-grid option needs nr nz dr dz"),
+    (["-R", "-CK"], "-CK option needs a checkpoint file name"),
+])
+def test_cli_rejects_malformed_option_values(flags, msg, tmp_path):
+    """This CLI's own options (-S, -T, -grid, -CK) report a malformed or
+    missing value, before any configuration is read or GPU used."""
+    sj, it = CONFIGS / "three_layer" / "sim_set.json", CONFIGS / "three_layer" / "input.txt"
+    r = run_cli(str(sj), str(it), "out.txt", *flags, cwd=str(tmp_path))
+    assert r.returncode == 0 and msg in r.stdout, (flags, r.stdout)
+    assert not any(tmp_path.iterdir())
+
+
 def test_cli_bad_config_exits_1():
     with tempfile.TemporaryDirectory() as td:
         sj, it = _write_case(td, dict(BASE, detector_reflectance=2.0), GOOD_INPUT)
