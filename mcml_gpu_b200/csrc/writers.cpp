@@ -35,34 +35,50 @@ std::string numbered(const char *prefix, int sds1, const char *postfix) {
 }
 
 // Text of lines [0, n) appended to fp.  line(i, p) writes line i at p (at
-// most max_line bytes) and returns its end.  Blocks of lines are formatted
-// by all host threads at once and written in order; per-line flushes of
-// the reference's `<< endl` only cost time, the bytes are the same.
+// most max_line bytes) and returns its end.  Lines go out in rounds: all
+// host threads format a round's blocks into one of two buffer sets while a
+// writer thread appends the previous round from the other set, so the file
+// output overlaps the formatting and the lines stay in order.  The
+// reference's per-line `<< endl` flushes only cost time; the bytes are the
+// same.
 template <class Line>
 bool append_lines(FILE *fp, size_t n, size_t max_line, Line line) {
   const size_t threads = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
   const size_t block = std::max<size_t>(1, (size_t(4) << 20) / max_line);
-  std::vector<std::string> buf(threads);
-  std::vector<size_t> used(threads);
-  for (size_t base = 0; base < n; base += threads * block) {
+  std::vector<std::string> buf[2] = {std::vector<std::string>(threads),
+                                     std::vector<std::string>(threads)};
+  std::vector<size_t> used[2] = {std::vector<size_t>(threads), std::vector<size_t>(threads)};
+  bool ok = true;  // set by the writer thread, read only after joining it
+  std::thread writer;
+  size_t round = 0;
+  for (size_t base = 0; base < n; base += threads * block, ++round) {
+    const int k = (int)(round & 1);
     auto work = [&](size_t t) {
       const size_t i0 = base + t * block, i1 = std::min(n, i0 + block);
-      used[t] = 0;
+      used[k][t] = 0;
       if (i0 >= i1) return;
-      buf[t].resize((i1 - i0) * max_line);
-      char *p = &buf[t][0];
+      buf[k][t].resize((i1 - i0) * max_line);
+      char *p = &buf[k][t][0];
       for (size_t i = i0; i < i1; ++i) p = line(i, p);
-      used[t] = (size_t)(p - &buf[t][0]);
+      used[k][t] = (size_t)(p - &buf[k][t][0]);
     };
     const size_t active = std::min(threads, (n - base + block - 1) / block);
     std::vector<std::thread> pool;
     for (size_t t = 1; t < active; ++t) pool.emplace_back(work, t);
     work(0);
     for (auto &th : pool) th.join();
-    for (size_t t = 0; t < active; ++t)
-      if (used[t] && std::fwrite(buf[t].data(), 1, used[t], fp) != used[t]) return false;
+    if (writer.joinable()) writer.join();  // the previous round is in the file
+    if (!ok) break;
+    writer = std::thread([&, k, active] {
+      for (size_t t = 0; t < active; ++t)
+        if (used[k][t] && std::fwrite(buf[k][t].data(), 1, used[k][t], fp) != used[k][t]) {
+          ok = false;
+          return;
+        }
+    });
   }
-  return true;
+  if (writer.joinable()) writer.join();
+  return ok;
 }
 
 }  // namespace

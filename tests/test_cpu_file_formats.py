@@ -150,3 +150,35 @@ def test_host_writer_matches_the_reference_formats(case, tmp_path):
     assert d["detect_mode"] == ("fiber" if sim.source_probe_oblique else "ring")
     assert d["SDS_detected_number"] == [len(r) for r in rows]
     assert '"SDS_detected_number": [ ' + " , ".join(str(len(r)) for r in rows) + " ]\n}" in text
+
+
+def test_large_text_file_keeps_row_order_across_write_rounds(tmp_path):
+    """A pathlength text file is formatted in rounds of up to 32 threads x
+    4 MB and written while the next round is formatted.  With 2.5e6 rows
+    (several rounds on any host) the file must equal the rows formatted in
+    order, twice after two appends; the single-threaded row formatter of the
+    library gives the expected bytes."""
+    import mcml_gpu_b200 as m
+    lib = m.load_library()
+    sim = load_case("ring5")
+    S, L = int(sim.num_sds), int(sim.num_layers)
+    rng = np.random.default_rng(11)
+    n = 2_500_000
+    big = (rng.random((n, L + 2)) * 5).astype(np.float32)
+    big[:, 0] = np.arange(1, n + 1, dtype=np.float32)  # row order is visible
+    rows = [big] + [np.zeros((0, L + 2), np.float32) for _ in range(S - 1)]
+    a_rz = np.zeros((S, 2, 2), np.uint64)
+    a0_z = np.zeros((S, 2), np.uint64)
+    wsum = np.zeros(S)
+    for _ in range(2):
+        _write(sim, 10**8, rows, a_rz, a0_z, wsum, (2, 2, 0.01, 0.01), tmp_path,
+               m.OUT_REPLAY | m.OUT_PATHLENGTH, 1.0, 1.0, "")
+    need = C.c_uint64(0)
+    assert lib.mcml_format_rows_text(big.ctypes.data, n, L + 2, None, 0, C.byref(need)) == 0
+    want = C.create_string_buffer(need.value)
+    assert lib.mcml_format_rows_text(big.ctypes.data, n, L + 2, want, need.value,
+                                     C.byref(need)) == 0
+    got = (tmp_path / "pathlength_SDS_1.txt").read_bytes()
+    assert len(got) == 2 * need.value
+    assert got == want.raw * 2
+    assert (tmp_path / "pathlength_SDS_2.txt").read_bytes() == b""
