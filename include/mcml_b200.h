@@ -224,6 +224,35 @@ int mcml_get_rows(mcml_ctx *ctx, int sds, float *rows, uint32_t *interactions,
  */
 int mcml_get_tallies(mcml_ctx *ctx, uint64_t *A_rz, uint64_t *A0_z);
 
+/*
+ * The last run's outputs where they lie, in device memory, for a caller that
+ * combines several GPUs' runs on the GPUs (sums of the u64 tallies and a
+ * gather of the rows over NCCL) instead of through host copies.  No
+ * counterpart in the reference (one GPU, host collection in
+ * transport.cu:274-332).  Records (and, after mcml_replay, rows) are put in
+ * file order first: SDS-major, photon order within an SDS, detected[s]
+ * entries for SDS s+1.  A record is 40 bytes: photon index u64, SDS u32,
+ * detected weight f32, the photon's XORWOW start state 6 x u32.  Rows are
+ * row_len = L+2 float32 in the pathlength_SDS_#.bin layout.  A_rz / A0_z are
+ * the u64 quanta of mcml_get_tallies.  Without a replay rows, A_rz and A0_z
+ * are NULL.  The pointers belong to the context: valid until its next run,
+ * replay, mcml_set_sim or mcml_destroy; work on them must be ordered after
+ * `stream` (the context's stream).  Synchronises that stream.
+ */
+typedef struct mcml_device_outputs {
+  const void *records;
+  const float *rows;
+  const uint64_t *A_rz;
+  const uint64_t *A0_z;
+  uint64_t n_records;
+  uint64_t detected[MCML_MAX_SDS];
+  uint64_t arz_count, a0z_count;
+  uint64_t photons;
+  uint32_t row_len;
+  void *stream;
+} mcml_device_outputs;
+int mcml_get_device_outputs(mcml_ctx *ctx, mcml_device_outputs *out);
+
 /* Replaces calculate_average_pathlength (transport.cu:274-297): out[S*L]. */
 int mcml_average_pathlength(mcml_ctx *ctx, double *out);
 
@@ -352,10 +381,10 @@ void mcml_mlp_destroy(mcml_mlp *mlp);
 /*
  * No counterpart in the reference (its host allocates with cudaMalloc on
  * every run, transport.cu:1037-1097).  For callers that cannot allocate
- * device memory when they want photons walked: code recording a CUDA graph
- * (allocation is not allowed during stream capture and would synchronise
- * the device), real-time pipelines whose device memory is fixed at
- * start-up, or processes whose GPU memory another framework's pool owns.
+ * device memory when they want photons walked: real-time pipelines whose
+ * device memory is fixed at start-up (cudaMalloc can block and synchronise
+ * the device mid-run), or processes whose GPU memory another framework's
+ * pool already owns.
  *
  * The walk's scratch memory is a fixed array of MCML_NOALLOC_SCRATCH_BYTES
  * inside the library, present on every GPU that loads it until the process
@@ -368,7 +397,8 @@ void mcml_mlp_destroy(mcml_mlp *mlp);
  * rejected with MCML_E_INVALID.  The same seed and slots give the same
  * counts as mcml_run.  No detection records are kept (use mcml_run for the
  * replay).  The first call on a device does its set-up (it looks up the
- * array's device address), so make that call before any stream capture.
+ * array's device address), and so does the first call after that device's
+ * context was reset; make that first call before any stream capture.
  * All calls share the one array, which keeps the last call's contents;
  * each call clears what must start at zero, and calls that overlap on the
  * GPU (different streams or host threads) race -- serialise them.

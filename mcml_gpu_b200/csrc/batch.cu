@@ -150,60 +150,15 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) batch_walk_kernel(const Ba
   if (!next_slot()) return;
   launch_photon<kSrcOblique>(p, &st, *tp, start_w);
   for (;;) {
-    const SmemTables &t = *tp;
-    float s;
-    const int new_layer = hop(p, s, &st, t);
-    p.steps++;
-    clamp_z(p, t, p.layer);
-    if (new_layer != p.layer) {
-      const int temp_layer = p.layer;
-      s = 0.0f;
-      if (!reflect(p, new_layer, &st, t)) {
-        if (new_layer == 0) {
-          bool detected = false;
-          const int base = b * 32;
-          if (kDetOblique) {
-            unsigned mask = fiber_mask(p, t, n_sds);
-            detected = mask != 0u;
-            while (mask) {
-              const int i = __ffs(mask) - 1;
-              mask &= mask - 1u;
-              atomicAdd(&A.det_count[base + i], 1ull);
-              atomicAdd(&A.wsum[base + i], (double)p.w);
-              atomicAdd(&A.wsq[base + i], (double)p.w * (double)p.w);
-            }
-          } else {
-            const float uz_angle = acosf(fabsf(p.dz));
-            const float distance = radius_xy(p);
-            for (int i = 1; i <= n_sds; i++) {
-              float wd;
-              if (ring_hit(p, t, i, uz_angle, distance, wd)) {
-                atomicAdd(&A.det_count[base + i], 1ull);
-                atomicAdd(&A.wsum[base + i], (double)wd);
-                atomicAdd(&A.wsq[base + i], (double)wd * (double)wd);
-                detected = true;
-              }
-            }
-          }
-          if (detected) {
-            p.w = 0;
-          } else if (uni(&st) > det_refl) {
-            p.w = 0;
-          } else {
-            p.dz *= -1;
-            p.z *= -1;
-            p.layer = temp_layer;
-          }
-        }
-        if (new_layer > n_layers) p.w = 0;
-      }
-    }
-    if (s > 0.0f) {
-      const float4 L = t.lay[p.layer];
-      drop_weight_walk(p, L.w);
-      spin(p, t.hg[p.layer], &st);
-    }
-    if (!survive<true>(p, &st)) {
+    const int base = b * 32;
+    const bool alive = walk_step<kDetOblique>(p, st, *tp, n_layers, n_sds, det_refl,
+                                              [&](int i, float w) {
+                                                atomicAdd(&A.det_count[base + i], 1ull);
+                                                atomicAdd(&A.wsum[base + i], (double)w);
+                                                atomicAdd(&A.wsq[base + i],
+                                                          (double)w * (double)w);
+                                              });
+    if (!alive) {
       steps_acc += (uint32_t)p.steps;
       const int prev_b = b;
       const bool slot_done = ++k >= quota;

@@ -164,59 +164,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
   launch_photon<kSrcOblique>(p, &st, t, P.start_weight);
 
   for (;;) {
-    // The photon's layer record, read once per step: hop, clamp and (when
-    // no boundary was hit, so the layer is unchanged) drop all use it.
-    const float4 L = t.lay[p.layer];
-    float s;
-    const int new_layer = hop(p, s, &st, L);
-    p.steps++;
-    clamp_z(p, L);
-
-    if (new_layer != p.layer) {
-      const int temp_layer = p.layer;
-      s = 0.0f;
-      if (!reflect(p, new_layer, &st, t)) {
-        if (new_layer == 0) {
-          bool detected = false;
-          if (kDetOblique) {
-            unsigned mask = fiber_mask(p, t, (int)P.n_sds);
-            detected = mask != 0u;
-            while (mask) {
-              const int i = __ffs(mask) - 1;
-              mask &= mask - 1u;
-              append_record(A, photon_index(), i, p.w, sc);
-            }
-          } else {
-            const float uz_angle = acosf(fabsf(p.dz));
-            const float distance = radius_xy(p);
-            for (int i = 1; i <= (int)P.n_sds; i++) {
-              float wd;
-              if (ring_hit(p, t, i, uz_angle, distance, wd)) {
-                append_record(A, photon_index(), i, wd, sc);
-                detected = true;
-              }
-            }
-          }
-          if (detected) {
-            p.w = 0;
-          } else if (uni(&st) > P.det_reflectance) {
-            p.w = 0;
-          } else {
-            p.dz *= -1;
-            p.z *= -1;
-            p.layer = temp_layer;
-          }
-        }
-        if (new_layer > (int)P.n_layers) p.w = 0;
-      }
-    }
-
-    if (s > 0.0f) {
-      drop_weight_walk(p, L.w);
-      spin(p, t.hg[p.layer], &st);
-    }
-
-    if (!survive<true>(p, &st)) {
+    const bool alive = walk_step<kDetOblique>(
+        p, st, t, (int)P.n_layers, (int)P.n_sds, P.det_reflectance,
+        [&](int i, float w) { append_record(A, photon_index(), i, w, sc); });
+    if (!alive) {
       const uint32_t acc = sc.steps[tid] + (uint32_t)p.steps;  // with the photon that just ended
       const uint32_t kk = ++sc.k[tid];
       const bool slot_done = kk >= sc.quota[tid];

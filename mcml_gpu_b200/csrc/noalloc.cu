@@ -1,16 +1,15 @@
 // noalloc.cu -- a first pass that allocates no device memory.
 //
 // Some callers cannot call cudaMalloc at the moment they want photons
-// walked: code that is recording a CUDA graph (an allocation is not allowed
-// while a stream is being captured, and it would synchronise the device), a
-// real-time pipeline whose device memory is fixed at start-up and must not
-// block in the allocator mid-run, or a process whose GPU memory is already
-// reserved by another framework's memory pool.  mcml_run_noalloc serves
-// them: the walk's scratch memory (slot cursor, per-SDS accumulators and
-// the XORWOW slot states) lives in the fixed array below, compiled into the
-// library, and the caller passes its inputs by value and a device buffer
-// for the outputs.  Nothing here calls cudaMalloc, cudaFree or any
-// allocating routine.
+// walked: a real-time pipeline whose device memory is fixed at start-up and
+// must not block in the allocator (cudaMalloc can synchronise the device)
+// mid-run, or a process whose GPU memory is already reserved by another
+// framework's memory pool, so that an allocation of its own would fail or
+// steal from that pool.  mcml_run_noalloc serves them: the walk's scratch
+// memory (slot cursor, per-SDS accumulators and the XORWOW slot states)
+// lives in the fixed array below, compiled into the library, and the caller
+// passes its inputs by value and a device buffer for the outputs.  Nothing
+// here calls cudaMalloc, cudaFree or any allocating routine.
 //
 // The array is MCML_NOALLOC_SCRATCH_BYTES (8 MiB) on every GPU that loads
 // the library, held until the process exits; it fits the reference's
@@ -18,6 +17,10 @@
 // it and it keeps the last call's contents: each call clears the part that
 // must start at zero, and calls that overlap on the GPU (two streams, two
 // host threads) race on it -- serialise them.
+//
+// The walk is the same step function (walk_step, photon.cuh) as the
+// allocating first pass; only where a detection goes differs (summed per
+// SDS here, appended as a record there).
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -25,8 +28,11 @@
 #include <mutex>
 #include <string>
 
+#include <cuda.h>  // CUcontext / CUresult types; the functions are looked up at run time
+
 #include "../../include/mcml_b200.h"
 #include "internal.h"
+#include "params.h"
 #include "photon.cuh"
 
 namespace mcml {
@@ -75,8 +81,8 @@ __device__ __forceinline__ void tally(Header *h, int sds, float w) {
   atomicAdd(&h->wsq[sds], (double)w * (double)w);
 }
 
-// The first pass of kernels.cu's walk_kernel with detections summed per
-// SDS in place of appended records.
+// The first pass (walk_step) with detections summed per SDS in place of
+// appended records.
 template <bool kSrcOblique, bool kDetOblique>
 __global__ void __launch_bounds__(128) noalloc_walk_kernel(const __grid_constant__ DevParams P,
                                                            unsigned char *scratch) {
@@ -116,54 +122,9 @@ __global__ void __launch_bounds__(128) noalloc_walk_kernel(const __grid_constant
   if (!next_slot()) return;
   launch_photon<kSrcOblique>(p, &st, t, P.start_weight);
   for (;;) {
-    float s;
-    const int new_layer = hop(p, s, &st, t);
-    p.steps++;
-    clamp_z(p, t, p.layer);
-    if (new_layer != p.layer) {
-      const int temp_layer = p.layer;
-      s = 0.0f;
-      if (!reflect(p, new_layer, &st, t)) {
-        if (new_layer == 0) {
-          bool detected = false;
-          if (kDetOblique) {
-            unsigned mask = fiber_mask(p, t, n_sds);
-            detected = mask != 0u;
-            while (mask) {
-              const int i = __ffs(mask) - 1;
-              mask &= mask - 1u;
-              tally(h, i, p.w);
-            }
-          } else {
-            const float uz_angle = acosf(fabsf(p.dz));
-            const float distance = radius_xy(p);
-            for (int i = 1; i <= n_sds; i++) {
-              float wd;
-              if (ring_hit(p, t, i, uz_angle, distance, wd)) {
-                tally(h, i, wd);
-                detected = true;
-              }
-            }
-          }
-          if (detected) {
-            p.w = 0;
-          } else if (uni(&st) > P.det_reflectance) {
-            p.w = 0;
-          } else {
-            p.dz *= -1;
-            p.z *= -1;
-            p.layer = temp_layer;
-          }
-        }
-        if (new_layer > n_layers) p.w = 0;
-      }
-    }
-    if (s > 0.0f) {
-      const float4 L = t.lay[p.layer];
-      drop_weight_walk(p, L.w);
-      spin(p, t.hg[p.layer], &st);
-    }
-    if (!survive<true>(p, &st)) {
+    const bool alive = walk_step<kDetOblique>(p, st, t, n_layers, n_sds, P.det_reflectance,
+                                              [&](int i, float w) { tally(h, i, w); });
+    if (!alive) {
       steps_acc += (uint32_t)p.steps;
       if (++k >= quota || steps_acc >= 0x40000000u) {
         atomicAdd(&h->steps, (unsigned long long)steps_acc);
@@ -190,15 +151,51 @@ __global__ void noalloc_finish_kernel(const unsigned char *scratch, unsigned n_s
 }
 
 // Per-device set-up: the device address of g_scratch (its host-side name is
-// only a stand-in) and the walk's launch shape.
+// only a stand-in: a kernel given it would fault or, where the GPU can reach
+// host memory, silently use the wrong memory) and the walk's launch shape.
+// It runs on the first call on a device, and again on the first call after
+// that device's context was replaced (cudaDeviceReset ends a context; the
+// next one loads the library's module anew, possibly at another address).
 struct DeviceSetup {
   bool done = false;
+  unsigned long long ctx_id = 0;  // context the address belongs to (0: unknown)
   unsigned char *scratch = nullptr;
   int grid[4] = {0, 0, 0, 0};
 };
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
 DeviceSetup g_setup[kMaxDevices];
+
+// Unique id of the calling thread's current CUDA context (cuCtxGetId ids
+// are never reused within a process), or 0 when there is none yet or the
+// driver lacks the call.  The driver functions are looked up through the
+// runtime, so the library does not link libcuda directly.
+unsigned long long current_context_id() {
+  using GetCurrent = CUresult (*)(CUcontext *);
+  using GetId = CUresult (*)(CUcontext, unsigned long long *);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  static bool looked_up = false;
+  if (!looked_up) {
+    cudaDriverEntryPointQueryResult q1, q2;
+    void *f1 = nullptr, *f2 = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) == cudaSuccess &&
+        q1 == cudaDriverEntryPointSuccess &&
+        cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) == cudaSuccess &&
+        q2 == cudaDriverEntryPointSuccess) {
+      get_current = reinterpret_cast<GetCurrent>(f1);
+      get_id = reinterpret_cast<GetId>(f2);
+    }
+    cudaGetLastError();
+    looked_up = true;
+  }
+  if (!get_current || !get_id) return 0;
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (get_current(&ctx) != CUDA_SUCCESS || ctx == nullptr) return 0;
+  if (get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
 
 const void *walk_fn(int variant) {
   switch (variant) {
@@ -209,10 +206,13 @@ const void *walk_fn(int variant) {
   }
 }
 
+// Called with `device` current.
 int setup_device(int device, DeviceSetup **out) {
   std::lock_guard<std::mutex> lock(g_setup_mutex);
   DeviceSetup &d = g_setup[device];
-  if (!d.done) {
+  const unsigned long long ctx = current_context_id();
+  if (!d.done || (ctx != 0 && ctx != d.ctx_id)) {
+    d.done = false;
     void *ptr = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&ptr, g_scratch);
     if (e != cudaSuccess)
@@ -230,6 +230,8 @@ int setup_device(int device, DeviceSetup **out) {
       d.grid[v] = (nb < 1 ? 1 : nb) * sms;
     }
     d.scratch = static_cast<unsigned char *>(ptr);
+    // the symbol lookup created the context if there was none yet
+    d.ctx_id = ctx != 0 ? ctx : current_context_id();
     d.done = true;
   }
   *out = &d;
@@ -274,36 +276,7 @@ extern "C" int mcml_run_noalloc(const mcml_sim *sim, uint64_t seed, uint64_t slo
   rc = setup_device(device, &d);
   if (rc == MCML_OK) {
     DevParams P;
-    std::memset(&P, 0, sizeof(P));
-    const int L = (int)sim->num_layers;
-    for (int l = 0; l <= L + 1; ++l) {
-      P.z_min[l] = der.z_min[l];
-      P.z_max[l] = der.z_max[l];
-      P.mutr[l] = der.mutr[l];
-      if (l >= 1 && l <= L) {
-        P.mua[l] = sim->mua[l - 1];
-        P.g[l] = sim->g[l - 1];
-        P.n[l] = sim->n[l - 1];
-      }
-    }
-    P.n[0] = sim->upper_n;
-    P.n[L + 1] = sim->lower_n;
-    P.det_radius[0] = sim->source_radius;
-    P.det_NA[0] = sim->source_NA;
-    P.det_angle[0] = der.det_angle_rad[0];
-    for (unsigned i = 0; i < sim->num_sds; ++i) {
-      P.det_radius[i + 1] = sim->det_radius[i];
-      P.det_NA[i + 1] = sim->det_NA[i];
-      P.det_pos[i + 1] = sim->det_pos[i];
-      P.det_angle[i + 1] = der.det_angle_rad[i + 1];
-      P.crit[i + 1] = der.critical_angle[i + 1];
-    }
-    P.n_layers = sim->num_layers;
-    P.n_sds = sim->num_sds;
-    P.start_weight = der.start_weight;
-    P.det_reflectance = sim->detector_reflectance;
-    P.num_photons = N;
-    P.num_slots = S;
+    fill_dev_params(*sim, der, N, S, P);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const int variant = (sim->source_probe_oblique ? 2 : 0) + (sim->detector_probe_oblique ? 1 : 0);
     noalloc_seed_kernel<<<(unsigned)((S + 255) / 256), 256, 0, s>>>(d->scratch, seed, S);

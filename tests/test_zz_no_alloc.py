@@ -1,7 +1,7 @@
 """mcml_run_noalloc: the first pass for callers that cannot allocate device
-memory (while recording a CUDA graph, in pipelines whose device memory is
-fixed at start-up, or when another framework's pool owns the GPU), with its
-scratch memory in a fixed array inside the library.
+memory (pipelines whose device memory is fixed at start-up, where cudaMalloc
+could block mid-run, or processes whose GPU memory another framework's pool
+owns), with its scratch memory in a fixed array inside the library.
 
 Called through the C ABI, twice in a row on the same fixed scratch array,
 it must give what mcml_run gives for the same seed and slot count: the
