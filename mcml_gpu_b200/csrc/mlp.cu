@@ -30,6 +30,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -214,6 +215,10 @@ cudaError_t gemm(const GemmArgs &g, int members, cudaStream_t s) {
 constexpr int TCM = 128;            // rows per tile (UMMA M)
 constexpr int kLboA = (TCM / 8) * 128;
 constexpr long long kTcSpin = 1ll << 22;
+// Polls of the end-of-kernel drain waits: those wait only for copies and
+// MMAs this CTA already issued, which finish in bounded time, so their
+// limit is far above the per-stage one and independent of it.
+constexpr long long kTcDrainSpin = 1ll << 26;
 
 enum TcEpi {
   kTcBiasGelu = 0,  // H = bf16(gelu(acc + b)), Z = acc + b (optional)
@@ -237,6 +242,7 @@ struct TcArgs {
   bf16 *H;                  // kTcBiasGelu: activations
   long long ldh, strideH;
   unsigned *status;
+  long long spin;           // polls per pipeline wait before it gives up (timeout)
   int slots;                // A ring slots (chunks of up to 64 K columns), 2..16
   int splits;               // K split over gridDim.z (member = z / splits, slice = z % splits)
   long long sliceA, sliceW; // element offsets of one K slice in A and W
@@ -267,8 +273,9 @@ __device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr) {
   return d;
 }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
-  for (long long i = 0; i < kTcSpin; ++i) {
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase,
+                                          long long limit = kTcSpin) {
+  for (long long i = 0; i < limit; ++i) {
     uint32_t done;
     asm volatile(
         "{\n .reg .pred P;\n mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n"
@@ -377,7 +384,12 @@ __device__ __forceinline__ void umma_commit(uint32_t bar) {
 // (acc_full) with tcgen05.commit; warps 4-11 drain an accumulator (bias,
 // GELU, stores) while the next tile's MMAs run, and hand it back
 // (acc_empty).  Every wait is bounded: a timeout sets *status and ends the
-// waiting role; the others then run out of their own waits.
+// waiting role; the others then run out of their own waits.  Whatever ends
+// the roles, the CTA drains its asynchronous work before it frees tensor
+// memory and exits: the TMA producer waits until every A load it issued has
+// landed (a load's a_full phase completes when its bytes arrive), the MMA
+// issuer commits all MMAs it issued to the drain barrier and waits for it,
+// cp.async copies are waited for and the epilogue's TMA stores are read out.
 constexpr int kTcWarps = 12;
 constexpr int kProducers = 96;  // warps 0-2
 
@@ -407,12 +419,13 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1)
   const size_t stage_bytes = g.use_tma_h ? (size_t)8 * 2 * 2048 : 0;
   float *sBias = reinterpret_cast<float *>(sStage + stage_bytes);
   uint64_t *bars = reinterpret_cast<uint64_t *>(sBias + 256);
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 36);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 37);
   const uint32_t sA_u = smem_u32(sA), sB_u = smem_u32(sB), bars_u = smem_u32(bars);
   auto a_full = [&](int s) { return bars_u + 8u * s; };
   auto a_empty = [&](int s) { return bars_u + 8u * (16 + s); };
   auto acc_full = [&](int b) { return bars_u + 8u * (32 + b); };
   auto acc_empty = [&](int b) { return bars_u + 8u * (34 + b); };
+  const uint32_t drain_bar = bars_u + 8u * 36;  // completion of every MMA issued
   const uint32_t need = 2u * (uint32_t)N;
   const uint32_t ncols = need <= 32 ? 32 : need <= 64 ? 64 : need <= 128 ? 128 : need <= 256 ? 256 : 512;
 
@@ -425,6 +438,7 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1)
       mbar_init(acc_full(b), 1);
       mbar_init(acc_empty(b), 256);
     }
+    mbar_init(drain_bar, 1);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   if (warp == 0) {
@@ -480,12 +494,12 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1)
     // rows, 128-byte swizzled, counted on a_full by its byte total; rows
     // past M read as zeros.  Coordinates: (K offset, row, member).
     if (tid == 0) {
-      int gi = 0;
+      int gi = 0;  // after the loop: the number of loads issued
       bool alive = true;
       for (int tile = blockIdx.x; tile < tiles && alive; tile += gridDim.x) {
         for (int c = 0; c < nch; ++c, ++gi) {
           const int slot = gi % nslots, use = gi / nslots;
-          if (use > 0 && !mbar_wait(a_empty(slot), (uint32_t)((use - 1) & 1))) {
+          if (use > 0 && !mbar_wait(a_empty(slot), (uint32_t)((use - 1) & 1), g.spin)) {
             atomicOr(g.status, 1u);
             alive = false;
             break;
@@ -501,6 +515,13 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1)
               "r"(tile * TCM), "r"(z)
               : "memory");
         }
+      }
+      // Drain: the last load issued into each slot has landed once that
+      // use's a_full phase is complete (already so if the MMAs consumed it).
+      for (int slot = 0; slot < nslots && slot < gi; ++slot) {
+        const int last_use = (gi - 1 - slot) / nslots;
+        if (!mbar_wait(a_full(slot), (uint32_t)(last_use & 1), kTcDrainSpin))
+          atomicOr(g.status, 2u);
       }
     }
     __syncwarp();
@@ -518,7 +539,7 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1)
       bool alive = true;
       for (int c = 0; c < nch; ++c, ++gi) {
         const int slot = gi % nslots, use = gi / nslots;
-        if (use > 0 && !mbar_wait(a_empty(slot), (uint32_t)((use - 1) & 1))) {
+        if (use > 0 && !mbar_wait(a_empty(slot), (uint32_t)((use - 1) & 1), g.spin)) {
           atomicOr(g.status, 1u);
           alive = false;
           break;
@@ -567,7 +588,7 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1)
       int t = 0;
       for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++t) {
         const int b = t & 1, u = t >> 1;
-        if (u > 0 && !mbar_wait(acc_empty(b), (uint32_t)((u - 1) & 1))) {
+        if (u > 0 && !mbar_wait(acc_empty(b), (uint32_t)((u - 1) & 1), g.spin)) {
           atomicOr(g.status, 1u);
           break;
         }
@@ -576,7 +597,7 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1)
         bool ok = true;
         for (int c = 0; c < nch && ok; ++c) {
           const int gi = t * nch + c, slot = gi % nslots, use = gi / nslots;
-          if (!mbar_wait(a_full(slot), (uint32_t)(use & 1))) {
+          if (!mbar_wait(a_full(slot), (uint32_t)(use & 1), g.spin)) {
             atomicOr(g.status, 1u);
             ok = false;
             break;
@@ -600,6 +621,9 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1)
         if (!ok) break;
         umma_commit(acc_full(b));
       }
+      // Drain: the commit tracks every MMA this thread issued before it.
+      umma_commit(drain_bar);
+      if (!mbar_wait(drain_bar, 0u, kTcDrainSpin)) atomicOr(g.status, 2u);
     }
     __syncwarp();
   } else {
@@ -610,7 +634,7 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1)
     for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++t) {
       const int b = t & 1, u = t >> 1;
       // whole warps or none: tcgen05.ld is warp-collective
-      if (!__all_sync(0xffffffffu, mbar_wait(acc_full(b), (uint32_t)(u & 1)))) {
+      if (!__all_sync(0xffffffffu, mbar_wait(acc_full(b), (uint32_t)(u & 1), g.spin))) {
         atomicOr(g.status, 1u);
         break;
       }
@@ -717,7 +741,7 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1)
 }
 
 constexpr size_t kTcSmemMax = 227 * 1024;  // opt-in shared memory per block
-constexpr size_t kTcSmemFixed = 256 * 4 + 36 * 8 + 16;  // bias, barriers, TMEM slot
+constexpr size_t kTcSmemFixed = 256 * 4 + 37 * 8 + 16;  // bias, barriers, TMEM slot
 
 size_t tc_slot_bytes(int K) { return (size_t)(K < 64 ? K : 64) / 8 * kLboA; }
 
@@ -801,6 +825,7 @@ cudaError_t tc_layer(const TcArgs &g, int members, cudaStream_t s) {
   if (g.N % 16 || g.N < 16 || g.N > 256 || g.K % 16 || g.K < 16 || g.K > 256 || g.n_valid > g.N)
     return cudaErrorInvalidValue;
   TcArgs a = g;
+  if (a.spin <= 0) a.spin = kTcSpin;
   CUtensorMap hmap;
   std::memset(&hmap, 0, sizeof(hmap));
   const bool stage = (EPI == kTcBiasGelu || EPI == kTcGeluBack) && (g.N / 2) % 32 == 0 &&
@@ -957,6 +982,10 @@ struct mcml_mlp {
   long long per_member = 0;        // parameters per member
   long long stride = 0;            // per_member rounded up to 8 (16-byte aligned BF16 blocks)
   unsigned *d_status = nullptr;    // tensor-core kernel timeouts
+  // Polls per pipeline wait of the tensor-core kernel before it gives up:
+  // kTcSpin, or MCML_MLP_WAIT_POLLS read once when the network is created
+  // (a test sets it tiny to make the waits run out on purpose).
+  long long spin = kTcSpin;
   float *d_w = nullptr;            // E x stride FP32 master (weights then biases per layer)
   float *d_m = nullptr, *d_v = nullptr, *d_g = nullptr;
   bf16 *d_w16 = nullptr;           // BF16 mirror (same layout)
@@ -1051,6 +1080,7 @@ int forward(mcml_mlp *p, int n, bool keep_z, bool shared_x = false) {
     g.bias = p->d_w + p->b_off[l];
     g.strideBias = P;
     g.status = p->d_status;
+    g.spin = p->spin;
     if (l < p->depth) {
       g.Z = keep_z ? p->d_z + (long long)l * cap * H : nullptr;
       g.ldz = H;
@@ -1076,7 +1106,13 @@ int check_status(mcml_mlp *p) {
   MLP_TRY(cudaStreamSynchronize(p->stream));
   if (st) {
     MLP_TRY(cudaMemset(p->d_status, 0, sizeof(unsigned)));
-    return set_error(MCML_E_BUDGET, "a tensor-core MMA did not complete in time");
+    // bit 0: a pipeline wait gave up (the layer's tiles are incomplete);
+    // bit 1: even the end-of-kernel drain of issued copies and MMAs did
+    if (st & 2u)
+      return set_error(MCML_E_BUDGET, "tensor-core kernel: a pipeline wait and the drain of "
+                                      "its issued copies and MMAs timed out");
+    return set_error(MCML_E_BUDGET, "tensor-core kernel: a pipeline wait timed out "
+                                    "(issued copies and MMAs drained)");
   }
   return MCML_OK;
 }
@@ -1117,6 +1153,7 @@ int backward(mcml_mlp *p, int n) {
       w.strideZ = P;
       w.splits = n / 256;
       w.status = p->d_status;
+      w.spin = p->spin;
       MLP_TRY((tc_layer<kTcAddF32, false, true>(w, p->E, p->stream)));
     } else {
     GemmArgs g;
@@ -1171,6 +1208,7 @@ int backward(mcml_mlp *p, int n) {
       t.ldh = H;
       t.strideH = cap * std::max<long long>(H, p->out_dim);
       t.status = p->d_status;
+      t.spin = p->spin;
       MLP_TRY((tc_layer<kTcGeluBack, true>(t, p->E, p->stream)));
       std::swap(dcur, dnext);
       dcur_ld = H;
@@ -1217,6 +1255,10 @@ int mcml_mlp_create(const mcml_mlp_config *cfg, mcml_mlp **out) {
                      "at most 256; out_dim <= hidden)");
   std::unique_ptr<mcml_mlp> p(new mcml_mlp());
   p->device = cfg->device;
+  if (const char *e = std::getenv("MCML_MLP_WAIT_POLLS")) {
+    const long long v = std::atoll(e);
+    if (v > 0) p->spin = v;
+  }
   MlpGuard gd(cfg->device);
   p->in_dim = cfg->in_dim;
   p->in_pad = (cfg->in_dim + 15) / 16 * 16;

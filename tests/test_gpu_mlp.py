@@ -167,3 +167,31 @@ def test_tensor_arguments_are_checked(gpu_available):
         mlp.train_epoch(X, T[:32], batch=32)
     mean, spread = mlp.predict(X)  # the checked path still runs
     assert mean.shape == (64, 3) and spread.shape == (64, 3)
+
+
+@pytest.mark.gpu
+def test_pipeline_wait_timeout_is_reported_and_drained(gpu_available, monkeypatch):
+    """Every wait of the tensor-core kernel is bounded.  With the bound cut
+    to one poll (MCML_MLP_WAIT_POLLS, read when a network is created) the
+    waits run out on purpose: predict() must return MCML_E_BUDGET after the
+    kernel drained what it had issued (bit 1 of the status word, a failed
+    drain, must stay clear), and the context must stay usable -- a network
+    created afterwards with the normal bound predicts what a fresh one does."""
+    from mcml_gpu_b200 import MCMLError
+    rng = np.random.default_rng(11)
+    n = 65536
+    X = torch.from_numpy(rng.normal(size=(n, 25)).astype(np.float32)).cuda()
+    monkeypatch.setenv("MCML_MLP_WAIT_POLLS", "1")
+    tiny = sg.MLP(25, 3, hidden=256, depth=4, ensemble=2, seed=5)
+    monkeypatch.delenv("MCML_MLP_WAIT_POLLS")
+    with pytest.raises(MCMLError) as err:
+        tiny.predict(X)
+    assert err.value.status == -8  # MCML_E_BUDGET
+    assert "drained" in err.value.message, err.value.message
+    tiny.close()
+    a = sg.MLP(25, 3, hidden=256, depth=4, ensemble=2, seed=5)
+    b = sg.MLP(25, 3, hidden=256, depth=4, ensemble=2, seed=5)
+    ma, sa = a.predict(X)
+    mb, sb = b.predict(X)
+    assert torch.equal(ma, mb) and torch.equal(sa, sb)
+    assert bool(torch.isfinite(ma).all())
