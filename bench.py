@@ -15,8 +15,15 @@ launching stream, L2 flushed between steps); `e2e` times the same work
 through the public API from host structs to host result buffers.  The
 reference arm (`--impl reference`) times the CPU restatement of the
 reference algorithm (the reference has no CPU implementation) on all host
-cores over a bounded photon sample.  Under torchrun each rank walks its
-own subsequence range (weak scaling) and rank 0 prints one JSON line.
+cores over a bounded photon sample; it loads the oracle only, never this
+library.  Under torchrun each rank walks its own subsequence range (weak
+scaling) and rank 0 prints one JSON line.
+
+Beside the timed region, the line carries two baselines: `cpu_baseline`
+(the CPU restatement on the host cores) and `reference_cuda` (the
+reference's own CUDA build and this library's command line, each run as a
+whole process on the same input, `-R -A -B`, wall clock from start to
+exit).  Both are comparators; neither is part of the measured path.
 """
 from __future__ import annotations
 
@@ -140,6 +147,16 @@ def load_sim(photons: int | None):
     return sim
 
 
+def load_sim_oracle(photons: int | None = None):
+    """The benchmark tissue read by the oracle's own configuration reader
+    (the CPU legs load no part of this library)."""
+    import oracle
+    sim = oracle.read_config(CONFIG / "sim_set.json", CONFIG / "input.txt")[0]
+    if photons:
+        sim.number_photons = int(photons)
+    return sim
+
+
 def cpu_port_rate(sim, seconds: float, threads: int = 0) -> dict:
     """The CPU restatement (oracle, FP32, PCG32) timed on all host cores over a
     photon sample sized to take about `seconds`."""
@@ -162,7 +179,7 @@ def reference_arm(args) -> int:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    sim = load_sim(args.photons)
+    sim = load_sim_oracle(args.photons)
     cores = os.cpu_count() or 1
     # each step: a bounded sample of the workload on all cores
     import oracle
@@ -193,6 +210,89 @@ def reference_arm(args) -> int:
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def _timed_cli(cmd: list[str], workdir: Path, env: dict) -> tuple[float, dict]:
+    """One run of a MCML_GPU command line in `workdir` (fresh files), wall
+    clock from process start to exit; returns (seconds, its summary.json)."""
+    for f in workdir.iterdir():
+        if f.is_file() and f.name not in ("sim_set.json", "input.txt"):
+            f.unlink()
+    t0 = time.perf_counter()
+    res = subprocess.run(cmd, cwd=workdir, env=env, capture_output=True, text=True, timeout=1200)
+    dt = time.perf_counter() - t0
+    if res.returncode != 0:
+        raise RuntimeError(f"{cmd[0]} exited {res.returncode}: {(res.stdout + res.stderr)[-500:]}")
+    summ = {}
+    p = workdir / "summary.json"
+    if p.exists():
+        txt = p.read_text()
+        for key in ("sim_time", "replay_time"):
+            k = txt.find(f'"{key}": ')
+            if k >= 0:
+                summ[key] = float(txt[k + len(key) + 4:].split(",")[0])
+        k = txt.find('"SDS_detected_number": [')
+        if k >= 0:
+            body = txt[k + 24:txt.index("]", k)]
+            summ["detected"] = [int(v) for v in body.replace(",", " ").split()]
+    return dt, summ
+
+
+def reference_cuda_leg(photons: int, runs: int, seed: int) -> dict:
+    """The reference's own CUDA build against this library's command line,
+    like for like: `MCML_GPU sim_set.json input.txt output.txt -R -A -B` on
+    the benchmark tissue at `photons`, one process per run in a fresh
+    directory, wall clock from process start to exit (CUDA start-up, first
+    pass, replay and every output file included), one untimed run of each
+    first.  The reference (oracle/_ref/MCML_GPU, compiled from its own
+    sources for sm_100a) is seeded through the time() shim because it seeds
+    from time(NULL); this library's CLI takes -S.  `first_pass_s` is each
+    program's own sim_time from summary.json (the reference's is CPU
+    clock(), which its busy-waiting host loop keeps close to wall time)."""
+    import oracle
+    ours = ROOT / "mcml_gpu_b200" / "bin" / "MCML_GPU"
+    if not oracle.REF_BIN.exists() or not oracle.REF_SHIM.exists():
+        return {"unavailable": "oracle/_ref is not built"}
+    if not ours.exists():
+        return {"unavailable": "mcml_gpu_b200/bin/MCML_GPU is not built"}
+    conf = json.loads((CONFIG / "sim_set.json").read_text())
+    conf["number_photons"] = int(photons)
+    out = {"photons": int(photons), "runs": runs, "flags": "-R -A -B",
+           "timing": "wall clock per process, start to exit, after one untimed run"}
+    with tempfile.TemporaryDirectory() as td:
+        for name, cmd, env in (
+                ("reference", [str(oracle.REF_BIN)],
+                 dict(os.environ, MCML_FIXED_TIME=str(seed), LD_PRELOAD=str(oracle.REF_SHIM))),
+                ("this_library", [str(ours)], dict(os.environ))):
+            wd = Path(td) / name
+            wd.mkdir()
+            (wd / "sim_set.json").write_text(json.dumps(conf))
+            (wd / "input.txt").write_text((CONFIG / "input.txt").read_text())
+            full = cmd + ["sim_set.json", "input.txt", "output.txt", "-R", "-A", "-B"]
+            if name == "this_library":
+                full += ["-S", str(seed)]
+            try:
+                _timed_cli(full, wd, env)
+                walls, firsts, det = [], [], None
+                for _ in range(runs):
+                    dt, summ = _timed_cli(full, wd, env)
+                    walls.append(dt)
+                    if "sim_time" in summ:
+                        firsts.append(summ["sim_time"])
+                    det = summ.get("detected", det)
+            except Exception as e:  # report, do not fail the bench line
+                out[name] = {"unavailable": str(e)[:300]}
+                continue
+            wall = statistics.median(walls)
+            out[name] = {"wall_s": wall, "wall_s_runs": walls, "photons_per_s": photons / wall,
+                         "first_pass_s": statistics.median(firsts) if firsts else None,
+                         "detected": det}
+    if "wall_s" in out.get("reference", {}) and "wall_s" in out.get("this_library", {}):
+        out["speedup_wall"] = out["reference"]["wall_s"] / out["this_library"]["wall_s"]
+        fr, fo = out["reference"]["first_pass_s"], out["this_library"]["first_pass_s"]
+        if fr and fo:
+            out["speedup_first_pass"] = fr / fo
+    return out
 
 
 def reference_gpu_arm(args) -> int:
@@ -583,6 +683,11 @@ def mcml_arm(args) -> int:
     def step():
         run.launch_run()
         run.launch_replay()
+        if dist:
+            # the job's one exchange: u64 tallies summed and rows gathered over
+            # NCCL on the device buffers (rank 0 gets the whole run)
+            from mcml_gpu_b200.distributed import gather_device
+            gather_device(run.device_outputs())
 
     for _ in range(args.warmup):
         flush.zero_()
@@ -660,13 +765,17 @@ def mcml_arm(args) -> int:
         "config": {"workload": WORKLOAD, "photons": N, "layers": L, "sds": S,
                    "grid": "1000x500 @ 0.01 cm", "slots": int(res.slots),
                    "l2": "flushed between steps (256 MiB write)",
-                   "parallelism": f"replicas x{world}, disjoint RNG subsequences",
+                   "parallelism": (f"replicas x{world}, disjoint RNG subsequences; tallies "
+                                   f"all-reduced and rows all-gathered over NCCL in each step"
+                                   if world > 1 else "1 GPU"),
                    "steps_per_photon": round(steps_per_photon, 2),
                    "detected": [int(v) for v in res.detected[:S]],
                    "replayed_rows": int(sum(rep.detected[:S]))},
         "e2e": {"value": N * world / e2e_s, "unit": "photons/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": int(d2h)},
-        "gpu_launches": 4 * args.steps,
+        # seeding, walk, record reduction, replay; with ranks to combine also the
+        # record ordering (keys + gather; the radix sort between them is CUB's)
+        "gpu_launches": (4 + (2 if world > 1 else 0)) * args.steps,
         "roofline": {"bound": "issue", "achieved": achieved / 1e9, "peak": peak / 1e9,
                      "unit": "Gstep/s", "frac": achieved / peak,
                      "traffic": read_traffic(int(res.slots)),
@@ -681,9 +790,19 @@ def mcml_arm(args) -> int:
         "clocks": clocks,
         "wall_s_timed": wall,
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_port_rate(load_sim(None), args.cpu_seconds)
+    S = int(sim.num_sds)
+    line["reflectance"] = {
+        "per_sds": [float(v) for v in res.reflectance[:S]],
+        "std_error": [float(v) for v in res.std_error[:S]],
+        "detected": [int(v) for v in res.detected[:S]],
+        "photons": int(res.photons),
+        "note": "first pass of the last timed step: R_s = sum of detected weights / "
+                "(0xFFFFFFFF N), SE from the per-photon weight variance"}
     run.close()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_port_rate(load_sim_oracle(), args.cpu_seconds)
+    if rank == 0 and world == 1 and args.ref_cuda_runs > 0:
+        line["reference_cuda"] = reference_cuda_leg(N, args.ref_cuda_runs, args.seed)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -707,6 +826,8 @@ def main() -> int:
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-sample", type=int, default=300000)
+    ap.add_argument("--ref-cuda-runs", type=int, default=3,
+                    help="timed runs of each CLI in the reference_cuda leg (0: skip it)")
     ap.add_argument("--sets", type=int, default=4096)
     ap.add_argument("--min-photons", type=float, default=1e5)
     ap.add_argument("--max-photons", type=float, default=1e7)

@@ -13,6 +13,8 @@ from pathlib import Path
 
 import numpy as np
 
+from .config import ConfigError, Derived, Sim, read_config  # noqa: F401
+
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "_build" / "liboracle.so"
 REF_BIN = HERE / "_ref" / "MCML_GPU"
@@ -68,8 +70,7 @@ def _p(a):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
 
 
-def derive(sim) -> "object":
-    from mcml_gpu_b200 import Derived  # struct layout only
+def derive(sim) -> Derived:
     d = Derived()
     load().oracle_derive(C.byref(sim), C.byref(d))
     return d

@@ -52,3 +52,27 @@ def test_reference_arm_other_ranks_print_nothing(rank):
     p = _run({"RANK": rank, "WORLD_SIZE": "4"})
     assert p.returncode == 0, p.stderr[-2000:]
     assert p.stdout.strip() == ""
+
+
+def test_reference_arm_loads_only_the_oracle():
+    """`bench.py --impl reference` times the CPU restatement; it must not
+    import this library's Python package nor map its shared library (it
+    reads the configuration with the oracle's own reader)."""
+    import subprocess
+    import sys
+    code = (
+        "import runpy, sys\n"
+        "sys.argv = ['bench.py', '--impl', 'reference', '--steps', '1', '--warmup', '0',"
+        " '--ref-sample', '2000']\n"
+        "try:\n    runpy.run_path('bench.py', run_name='__main__')\n"
+        "except SystemExit:\n    pass\n"
+        "maps = open('/proc/self/maps').read()\n"
+        "print('PRODUCT', 'libmcml_b200' in maps, 'mcml_gpu_b200' in sys.modules)\n"
+        "print('ORACLE', 'liboracle' in maps)\n")
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert "PRODUCT False False" in r.stdout, r.stdout
+    assert "ORACLE True" in r.stdout, r.stdout
+    line = [ln for ln in r.stdout.splitlines() if ln.startswith("{")][0]
+    assert '"impl": "reference"' in line
