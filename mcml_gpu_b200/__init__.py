@@ -145,6 +145,23 @@ class DeviceInfo(C.Structure):
     ]
 
 
+class DeviceOutputs(C.Structure):
+    """mcml_device_outputs: a run's outputs in device memory."""
+    _fields_ = [
+        ("records", C.c_void_p),
+        ("rows", C.c_void_p),
+        ("A_rz", C.c_void_p),
+        ("A0_z", C.c_void_p),
+        ("n_records", C.c_uint64),
+        ("detected", C.c_uint64 * MAX_SDS),
+        ("arz_count", C.c_uint64),
+        ("a0z_count", C.c_uint64),
+        ("photons", C.c_uint64),
+        ("row_len", C.c_uint32),
+        ("stream", C.c_void_p),
+    ]
+
+
 class NoallocResult(C.Structure):
     """mcml_noalloc_result, written to device memory by mcml_run_noalloc."""
     _fields_ = [
@@ -233,6 +250,7 @@ _SIGNATURES = [
     ("mcml_get_rows", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_uint64,
                                 C.POINTER(C.c_uint64)]),
     ("mcml_get_tallies", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("mcml_get_device_outputs", C.c_int, [C.c_void_p, C.POINTER(DeviceOutputs)]),
     ("mcml_average_pathlength", C.c_int, [C.c_void_p, C.c_void_p]),
     ("mcml_write_outputs", C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_uint32,
                                      C.c_double, C.c_double]),
@@ -540,6 +558,37 @@ class Simulation:
                                           a0z.ctypes.data_as(C.c_void_p)), "mcml_get_tallies")
         return arz, a0z
 
+    def device_outputs(self) -> dict:
+        """The last run's outputs as torch tensors on this context's GPU,
+        aliasing the library's memory (mcml_get_device_outputs): `records`
+        (D, 10) float32 words of the 40-byte records (word 3 is the detected
+        weight), `rows` (D, L+2) float32 or None, `A_rz` (S, nz, nr) and
+        `A0_z` (S, nz) int64 views of the u64 quanta or None, `detected`
+        (host list, per SDS), `photons`.  File order: SDS-major, photon
+        order within an SDS.  Valid until the context's next run, replay or
+        close; copy what must outlive that."""
+        import torch
+        o = DeviceOutputs()
+        _check(self._lib.mcml_get_device_outputs(self._ctx, C.byref(o)),
+               "mcml_get_device_outputs")
+        dev = torch.device("cuda", self.opts.device)
+        D, rl, S = int(o.n_records), int(o.row_len), self.num_sds
+        nr, nz, _, _ = self.grid
+
+        def view(ptr, shape, typestr):
+            if not ptr or any(d == 0 for d in shape):
+                return torch.zeros(shape, dtype=torch.float32 if typestr == "<f4" else torch.int64,
+                                   device=dev)
+            return torch.as_tensor(_CudaArray(ptr, shape, typestr), device=dev)
+        return {
+            "records": view(o.records, (D, 10), "<f4"),
+            "rows": view(o.rows, (D, rl), "<f4") if o.rows else None,
+            "A_rz": view(o.A_rz, (S, nz, nr), "<i8") if o.A_rz else None,
+            "A0_z": view(o.A0_z, (S, nz), "<i8") if o.A0_z else None,
+            "detected": [int(v) for v in o.detected[:S]],
+            "photons": int(o.photons),
+        }
+
     def average_pathlength(self) -> np.ndarray:
         out = np.empty(self.num_sds * self.num_layers, dtype=np.float64)
         _check(self._lib.mcml_average_pathlength(self._ctx, out.ctypes.data_as(C.c_void_p)),
@@ -567,6 +616,15 @@ class Simulation:
             self.close()
         except Exception:
             pass
+
+
+class _CudaArray:
+    """A device buffer of the library seen through __cuda_array_interface__,
+    so that torch.as_tensor wraps it without a copy."""
+
+    def __init__(self, ptr: int, shape: tuple, typestr: str):
+        self.__cuda_array_interface__ = {"data": (int(ptr), False), "shape": tuple(shape),
+                                         "typestr": typestr, "strides": None, "version": 2}
 
 
 class Batch:

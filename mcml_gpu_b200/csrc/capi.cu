@@ -252,10 +252,12 @@ int fill_result(mcml_ctx *c, mcml_result *r) {
 
 // Records (and, after a replay, rows and interaction counts) to the host
 // in file order: by SDS, then photon index -- sorted on the device.
-int fetch_host(mcml_ctx *c) {
-  if (c->host_valid) return MCML_OK;
+// The records (and, after a replay, rows and interaction counts) of the
+// last run put in file order on the device: SDS-major, photon order within
+// an SDS.  *D gets the record count; o points into the context's ordering
+// scratch (valid until the next ordering).  The caller holds the device.
+int order_on_device(mcml_ctx *c, uint64_t *D_out, OrderedOutput *o) {
   if (!c->ran) return set_error(MCML_E_STATE, "mcml_run has not been called");
-  DeviceGuard g(c->device);
   unsigned long long cnt[kCntWords];
   CUDA_TRY(cudaMemcpyAsync(cnt, c->d_counters, sizeof(cnt), cudaMemcpyDeviceToHost, c->stream));
   CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -266,9 +268,8 @@ int fetch_host(mcml_ctx *c) {
   const uint64_t D = cnt[kCntRecords];
   const int L = (int)c->sim.num_layers;
   const bool rows = c->replayed;
-  c->h_rec.resize(D);
-  c->h_rows.resize(rows ? D * (L + 2) : 0);
-  c->h_inter.resize(rows ? D * L : 0);
+  *D_out = D;
+  *o = OrderedOutput{};
   if (D) {
     // Ordering scratch: kept by the context and grown, never shrunk.
     const size_t need = order_scratch_bytes(D, L, rows);
@@ -278,9 +279,26 @@ int fetch_host(mcml_ctx *c) {
       CUDA_TRY(cudaMalloc(&c->d_order, need));
       c->order_bytes = need;
     }
-    OrderedOutput o;
     CUDA_TRY(sort_records_for_output(c->d_records, D, rows ? c->d_rows : nullptr, c->d_inter, L,
-                                     c->d_order, c->order_bytes, &o, c->sm_count, c->stream));
+                                     c->d_order, c->order_bytes, o, c->sm_count, c->stream));
+  }
+  return MCML_OK;
+}
+
+int fetch_host(mcml_ctx *c) {
+  if (c->host_valid) return MCML_OK;
+  if (!c->ran) return set_error(MCML_E_STATE, "mcml_run has not been called");
+  DeviceGuard g(c->device);
+  uint64_t D = 0;
+  OrderedOutput o;
+  int rc = order_on_device(c, &D, &o);
+  if (rc) return rc;
+  const int L = (int)c->sim.num_layers;
+  const bool rows = c->replayed;
+  c->h_rec.resize(D);
+  c->h_rows.resize(rows ? D * (L + 2) : 0);
+  c->h_inter.resize(rows ? D * L : 0);
+  if (D) {
     CUDA_TRY(cudaMemcpyAsync(c->h_rec.data(), o.records, D * sizeof(DetRecord),
                              cudaMemcpyDeviceToHost, c->stream));
     if (rows) {
@@ -810,6 +828,34 @@ int mcml_get_tallies(mcml_ctx *ctx, uint64_t *A_rz, uint64_t *A0_z) {
     CUDA_TRY(cudaMemcpy(A_rz, ctx->d_Arz, ctx->arz_n * sizeof(uint64_t), cudaMemcpyDeviceToHost));
   if (A0_z)
     CUDA_TRY(cudaMemcpy(A0_z, ctx->d_A0z, ctx->a0z_n * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+  return MCML_OK;
+}
+
+int mcml_get_device_outputs(mcml_ctx *ctx, mcml_device_outputs *out) {
+  clear_error();
+  if (!ctx || !out) return set_error(MCML_E_INVALID, "null argument");
+  DeviceGuard g(ctx->device);
+  uint64_t D = 0;
+  OrderedOutput o;
+  int rc = order_on_device(ctx, &D, &o);
+  if (rc) return rc;
+  std::memset(out, 0, sizeof(*out));
+  unsigned long long cnt[32];
+  CUDA_TRY(cudaMemcpyAsync(cnt, ctx->d_sums, sizeof(cnt), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  for (unsigned s = 0; s < ctx->sim.num_sds; ++s) out->detected[s] = cnt[s];
+  out->records = o.records;
+  out->n_records = D;
+  out->row_len = ctx->sim.num_layers + 2;
+  out->photons = ctx->N;
+  if (ctx->replayed) {
+    out->rows = o.rows;
+    out->A_rz = reinterpret_cast<const uint64_t *>(ctx->d_Arz);
+    out->A0_z = reinterpret_cast<const uint64_t *>(ctx->d_A0z);
+    out->arz_count = ctx->arz_n;
+    out->a0z_count = ctx->a0z_n;
+  }
+  out->stream = ctx->stream;
   return MCML_OK;
 }
 

@@ -14,7 +14,12 @@ across ranks instead of across threads:
     same seed and slots byte for byte.
 
 `combine` does the same for shards held in one process (tests; one GPU
-walking the shards one after another).  Nothing here runs on the oracle.
+walking the shards one after another).  `gather_device` is the combine of
+a multi-GPU job: it runs the collectives on the tensors where they lie --
+under NCCL on each GPU's own device memory (Simulation.device_outputs), so
+the 12 MB of tallies and the rows cross NVLink, not the host -- and only
+rank 0's result comes to the host, for the writers.  `gather_to_rank0`
+is the host-array form (a gloo group).  Nothing here runs on the oracle.
 """
 from __future__ import annotations
 
@@ -27,7 +32,8 @@ import numpy as np
 
 from . import HostData, Sim, Simulation, _check, load_library
 
-__all__ = ["Shard", "slot_span", "run_shard", "combine", "gather_to_rank0", "write_outputs"]
+__all__ = ["Shard", "slot_span", "run_shard", "combine", "gather_to_rank0", "gather_device",
+           "write_outputs"]
 
 
 @dataclass
@@ -151,6 +157,67 @@ def gather_to_rank0(local: Shard, group=None) -> Optional[Shard]:
     if rank != 0:
         return None
     return Shard(int(meta[0]), weights, rows, tallies[0], tallies[1], int(meta[1]))
+
+
+def gather_device(out: dict, steps: int = 0, group=None) -> Optional[Shard]:
+    """The combine of a multi-GPU job over the ranks' device tensors.
+
+    Every rank calls this once, in the same order, with its own
+    Simulation.device_outputs() (or tensors of the same layout: `records`
+    (D, 10) float32 words, weight in word 3; `rows` (D, L+2) float32 or
+    None; `A_rz`, `A0_z` int64 or None; `detected` per SDS; `photons`), all
+    on one device per rank -- GPU tensors under NCCL, CPU tensors under gloo.
+      * A_rz, A0_z: one all-reduce (SUM) of the int64 views of the u64
+        quanta -- two's-complement sums are the u64 sums bit for bit;
+      * per-SDS counts, photons and steps: one all-gather;
+      * rows (without a replay, the records' weights): one all-gather of
+        every rank's D entries, padded to the largest D.
+    Rank 0 gets the whole run as host arrays in rank (= slot) order, the
+    photon order of one run over all slots; the other ranks get None."""
+    import torch
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    dev = out["records"].device
+    S = len(out["detected"])
+    meta = torch.tensor(list(out["detected"]) + [int(out["photons"]), int(steps)],
+                        dtype=torch.int64, device=dev)
+    metas = [torch.empty_like(meta) for _ in range(world)]
+    dist.all_gather(metas, meta, group=group)
+    counts = torch.stack(metas).cpu().numpy()  # (world, S + 2)
+    replay = out["rows"] is not None
+    flat = None
+    if replay:
+        flat = torch.cat([out["A_rz"].reshape(-1), out["A0_z"].reshape(-1)]).to(torch.int64)
+        dist.all_reduce(flat, group=group)
+    data = out["rows"] if replay else out["records"][:, 3:4]
+    D = int(data.shape[0])
+    if D != int(counts[rank, :S].sum()):
+        raise ValueError(f"rank {rank}: {D} entries but {counts[rank, :S].sum()} detections")
+    dmax = max(int(counts[:, :S].sum(axis=1).max()), 1)
+    pad = torch.zeros((dmax, data.shape[1]), dtype=torch.float32, device=dev)
+    pad[:D] = data
+    bufs = [torch.empty_like(pad) for _ in range(world)]
+    dist.all_gather(bufs, pad, group=group)
+    if rank != 0:
+        return None
+    host = [b.cpu().numpy() for b in bufs]
+    per_sds = []
+    for s in range(S):
+        parts = []
+        for r in range(world):
+            off = int(counts[r, :s].sum())
+            parts.append(host[r][off:off + int(counts[r, s])])
+        per_sds.append(np.concatenate(parts))
+    tallies = [None, None]
+    if replay:
+        k = out["A_rz"].numel()
+        f = flat.cpu().numpy().astype(np.uint64)
+        tallies = [f[:k].reshape(tuple(out["A_rz"].shape)), f[k:].reshape(tuple(out["A0_z"].shape))]
+    rows = per_sds if replay else None
+    weights = [r[:, 0].copy() for r in per_sds]
+    return Shard(int(counts[:, S].sum()), weights, rows, tallies[0], tallies[1],
+                 int(counts[:, S + 1].sum()))
 
 
 def write_outputs(sim: Sim, run: Shard, directory: str, output_txt: str, flags: int,

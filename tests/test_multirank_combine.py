@@ -76,6 +76,60 @@ def test_gather_to_rank0_equals_local_combine():
     assert got[4] == want.A_rz.tobytes() and got[5] == want.A0_z.tobytes()
 
 
+def device_layout(shard):
+    """A shard as Simulation.device_outputs() lays it out (CPU tensors here):
+    records SDS-major with the weight in word 3, rows likewise, int64 tallies."""
+    import torch
+    rows = np.concatenate(shard.rows)
+    rec = np.zeros((rows.shape[0], 10), np.float32)
+    rec[:, 3] = rows[:, 0]
+    return {"records": torch.from_numpy(rec), "rows": torch.from_numpy(rows),
+            "A_rz": torch.from_numpy(shard.A_rz.astype(np.int64)),
+            "A0_z": torch.from_numpy(shard.A0_z.astype(np.int64)),
+            "detected": [len(r) for r in shard.rows], "photons": shard.photons}
+
+
+def _rank_main_device(rank, world, port, out):
+    import datetime
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    from mcml_gpu_b200.distributed import gather_device
+    sh = synthetic_shard(rank)
+    got = gather_device(device_layout(sh), steps=sh.steps)
+    if rank == 0:
+        out.put((got.photons, got.steps, [w.tobytes() for w in got.weights],
+                 [r.tobytes() for r in got.rows], got.A_rz.tobytes(), got.A0_z.tobytes()))
+    else:
+        assert got is None
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_device_tensor_combine_equals_local_combine():
+    """gather_device -- the combine a multi-GPU job runs over NCCL on device
+    tensors -- on two gloo ranks with CPU tensors: rank 0 gets, byte for byte,
+    what combine() gives for the same shards in one process."""
+    from mcml_gpu_b200.distributed import combine
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main_device, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = q.get(timeout=120)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    want = combine([synthetic_shard(0), synthetic_shard(1)])
+    assert got[0] == want.photons == 2001 and got[1] == want.steps == 15
+    assert got[2] == [w.tobytes() for w in want.weights]
+    assert got[3] == [r.tobytes() for r in want.rows]
+    assert got[4] == want.A_rz.tobytes() and got[5] == want.A0_z.tobytes()
+
+
 def test_host_writer_files_carry_the_combined_run():
     import mcml_gpu_b200 as m
     from mcml_gpu_b200.distributed import combine, write_outputs
