@@ -17,7 +17,21 @@ for a few detected photons of each SDS, the first draws of their XORWOW
 subsequence (generated with curand on the GPU through the library's test
 entry point), so the CPU oracle can replay those photons with the
 reference's own random numbers.  A second, nondeterministic run at 4x the
-thread count gives the statistical fixture.
+thread count gives the statistical fixture.  The reference's summary.json
+of each run is stored too, for the drop-in test of the command line.
+
+Superset fixtures (``--superset five_layer:1000000000``): the reference
+at N well above its thread count T, where each thread walks about N/T
+photons and the split between threads depends on timing, but each
+thread's sequence of photons does not.  The fixture keeps every
+pathlength row the reference wrote; a run of this library with T slots of
+more photons than any thread walked must contain each of them bit for
+bit.
+
+Cases: fiber3, ring5, mismatch, ringpt (this build's geometries), three_layer
+(the 3-layer tissue with the README's fibres), surrogate (the 5-layer
+benchmark tissue with ring detectors), hw8a and head_model (the inputs the
+reference ships under example/HW8_A and example/head_model).
 """
 from __future__ import annotations
 
@@ -41,7 +55,9 @@ import oracle  # noqa: E402
 import mcml_gpu_b200 as mcml  # noqa: E402
 
 SEED = 20261203
-PARITY_CASES = ["fiber3", "ring5", "mismatch", "ringpt", "three_layer"]
+PARITY_CASES = ["fiber3", "ring5", "mismatch", "ringpt", "three_layer", "surrogate", "hw8a",
+                "head_model"]
+SUPERSET_CASES = "five_layer:1000000000"
 STREAM_PHOTONS_PER_SDS = 6
 
 
@@ -75,12 +91,36 @@ def summary_counts(path: Path) -> list[int]:
     return [int(v.strip()) for v in txt[i:j].split(",")]
 
 
+def superset_fixture(case: str, photons: int, T: int, out: Path, tmp: Path, seed: int) -> None:
+    """The reference at `photons` >> T with -R -P -B: counts, output.txt,
+    summary.json and every pathlength row, into superset_<case>.npz."""
+    cfg = HERE / "configs" / case
+    sim = mcml.parse_config(cfg / "sim_set.json", cfg / "input.txt")[0]
+    L, S = int(sim.num_layers), int(sim.num_sds)
+    wd = run_reference(case, photons, ["-R", "-P", "-B"], tmp / case / "superset", seed)
+    fx: dict[str, np.ndarray] = {
+        "seed": np.array(seed, dtype=np.uint64),
+        "threads": np.array(T, dtype=np.uint64),
+        "photons": np.array(photons, dtype=np.uint64),
+        "detected": np.array(summary_counts(wd / "summary.json"), dtype=np.uint64),
+        "output_txt": np.frombuffer((wd / "output.txt").read_bytes(), dtype=np.uint8),
+        "summary_json": np.frombuffer((wd / "summary.json").read_bytes(), dtype=np.uint8),
+    }
+    for s in range(1, S + 1):
+        fx[f"rows_{s}"] = np.fromfile(wd / f"pathlength_SDS_{s}.bin",
+                                      dtype=np.float32).reshape(-1, L + 2)
+    np.savez_compressed(out / f"superset_{case}.npz", **fx)
+    print(f"superset {case} at {photons}: detected {list(fx['detected'])}", flush=True)
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=str(HERE))
     ap.add_argument("--cases", default=",".join(PARITY_CASES))
     ap.add_argument("--seed", type=int, default=SEED)
     ap.add_argument("--keep", default="")
+    ap.add_argument("--superset", default=SUPERSET_CASES,
+                    help="case:photons[,case:photons...]; empty to skip")
     args = ap.parse_args()
     out = Path(args.out)
     out.mkdir(parents=True, exist_ok=True)
@@ -88,7 +128,10 @@ def main() -> int:
     T = int(info.reference_threads)
     print(f"device {info.name.decode()} reference threads {T}", flush=True)
     tmp = Path(args.keep) if args.keep else Path(tempfile.mkdtemp(prefix="golden_"))
-    for case in args.cases.split(","):
+    for item in filter(None, args.superset.split(",")):
+        case, photons = item.split(":")
+        superset_fixture(case, int(float(photons)), T, out, tmp, args.seed + 2)
+    for case in filter(None, args.cases.split(",")):
         cfg = HERE / "configs" / case
         sim = mcml.parse_config(cfg / "sim_set.json", cfg / "input.txt")[0]
         L, S = int(sim.num_layers), int(sim.num_sds)
@@ -100,6 +143,7 @@ def main() -> int:
         counts = summary_counts(wb / "summary.json")
         fx["detected"] = np.array(counts, dtype=np.uint64)
         fx["output_txt"] = np.frombuffer((wb / "output.txt").read_bytes(), dtype=np.uint8)
+        fx["summary_json"] = np.frombuffer((wb / "summary.json").read_bytes(), dtype=np.uint8)
         fx["average_pathlength_txt"] = np.frombuffer(
             (wb / "average_pathlength.txt").read_bytes(), dtype=np.uint8)
         for s in range(1, S + 1):
@@ -119,6 +163,7 @@ def main() -> int:
             head = b"".join((wt / f"pathlength_SDS_{s}.txt").read_bytes().splitlines(True)[:20])
             fx[f"pathlength_SDS_{s}_txt_head"] = np.frombuffer(head, dtype=np.uint8)
         fx["output_txt_textmode"] = np.frombuffer((wt / "output.txt").read_bytes(), np.uint8)
+        fx["summary_json_textmode"] = np.frombuffer((wt / "summary.json").read_bytes(), np.uint8)
         # draws of a few detected photons, located with the library at N == T
         sim.number_photons = T
         with mcml.Simulation(sim, seed=args.seed, slots=T) as run:

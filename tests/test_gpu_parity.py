@@ -30,6 +30,16 @@ import mcml_gpu_b200 as m
 
 GOLDEN_DIR = Path(os.environ.get("MCML_GOLDEN_DIR", GOLDEN))
 CASES = ["fiber3", "ring5", "mismatch", "ringpt", "three_layer"]
+STAT_CASES = ["fiber3", "ring5", "mismatch", "ringpt"]
+
+
+def same_or_both_nan(a: float, b: float, tol: float) -> bool:
+    """|a - b| <= tol, or both NaN: the reference's ring detector at pos = 0
+    (example/HW8_A) divides by 2*d*pos = 0 and records NaN weights
+    (transport.cu:915), which every sum over that SDS carries."""
+    if np.isnan(a) or np.isnan(b):
+        return bool(np.isnan(a) and np.isnan(b))
+    return abs(a - b) <= tol
 
 
 def golden(case):
@@ -102,9 +112,11 @@ def test_tallies_and_files_match_reference(case, gpu_available):
         np.testing.assert_allclose(out, exact, rtol=5e-6, atol=0)
         for i in range(S):
             n = g[f"rows_{i + 1}"].shape[0]
-            assert abs(out[i] - ref[i]) <= (n * 2.0 ** -24 + 1e-5) * abs(ref[i]), (i, out[i], ref[i])
+            assert same_or_both_nan(out[i], ref[i], (n * 2.0 ** -24 + 1e-5) * abs(ref[i])), \
+                (i, out[i], ref[i])
         for i in range(S):
-            assert abs(rep.weight_sum[i] - exact[i] * scale) <= 1e-12 * exact[i] * scale
+            assert same_or_both_nan(rep.weight_sum[i], exact[i] * scale,
+                                    1e-12 * abs(exact[i]) * scale), (i, rep.weight_sum[i])
 
 
 @pytest.mark.gpu
@@ -122,7 +134,7 @@ def test_text_mode_files_match_reference(case, gpu_available):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", ["fiber3", "ring5", "mismatch", "ringpt"])
+@pytest.mark.parametrize("case", STAT_CASES)
 def test_reflectance_within_3_se_of_reference_at_4x_threads(case, gpu_available):
     """At N = 4 x threads the reference's photon split is timing-dependent;
     reflectance must agree within 3 combined standard errors."""
@@ -135,7 +147,8 @@ def test_reflectance_within_3_se_of_reference_at_4x_threads(case, gpu_available)
     ref_R = [float(v) for v in bytes(g["stat_output_txt"]).decode().split()]
     for i in range(sim.num_sds):
         se = r.std_error[i] * np.sqrt(2.0)  # both estimates carry the same SE
-        assert abs(r.reflectance[i] - ref_R[i]) <= 3 * se + 1e-15, (i, r.reflectance[i], ref_R[i], se)
+        assert same_or_both_nan(r.reflectance[i], ref_R[i], 3 * se + 1e-15), \
+            (i, r.reflectance[i], ref_R[i], se)
 
 
 @pytest.mark.gpu
@@ -157,3 +170,96 @@ def test_rows_independent_of_launch_shape(case, shape, gpu_available):
         for sds in range(1, sim.num_sds + 1):
             rows, _ = s.rows(sds)
             assert rows.tobytes() == g[f"rows_{sds}"].tobytes(), f"SDS {sds}"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", STAT_CASES)
+def test_reflectance_within_3_se_of_fp64_host_build(case, gpu_available):
+    """The CUDA walk (FP32, XORWOW) against the FP64 host build of the same
+    walk (the oracle: double precision throughout, its own PCG32 stream per
+    photon) at 4 x threads photons each: per-SDS reflectance within 3
+    combined standard errors, each side's SE from its per-photon
+    detected-weight variance."""
+    import oracle
+    g = golden(case)
+    sim = load_case(case)
+    N = int(g["stat_photons"])
+    sim.number_photons = N
+    with m.Simulation(sim, seed=int(g["seed"]) + 3, slots=int(g["threads"])) as s:
+        r = s.run()
+    st, *_ = oracle.run(sim, N, 97, fp64=True)
+    W = 4294967295.0
+    for i in range(sim.num_sds):
+        R64 = st.wsum[i] / (W * N)
+        mean = st.wsum[i] / N
+        se64 = np.sqrt(max(st.wsq[i] / N - mean * mean, 0.0) / (N - 1)) / W
+        se = np.hypot(r.std_error[i], se64)
+        assert same_or_both_nan(r.reflectance[i], R64, 3 * se + 1e-15), \
+            (i, r.reflectance[i], R64, se)
+
+
+def superset(case):
+    p = GOLDEN_DIR / f"superset_{case}.npz"
+    if not p.exists():
+        pytest.fail(f"missing golden fixture {p}")
+    return np.load(p)
+
+
+@pytest.mark.gpu
+def test_benchmark_tissue_rows_of_reference_found_bit_exact(gpu_available):
+    """The 5-layer benchmark tissue (config 1), its three oblique fibres, at
+    1e9 photons.  The reference walked them on T threads (about N/T photons
+    each; which thread takes the last photons depends on timing, but each
+    thread's sequence of photons -- subsequence t, one photon after another
+    -- does not).  This library walks the same T subsequences with 1.5 N/T
+    photons each (slots = T), more than any reference thread walked, so:
+      * every pathlength row the reference wrote is among this run's rows,
+        bit for bit (weight, per-layer pathlengths, steps);
+      * every detection of this run among the first N/(4T) photons of its
+        slot -- photons every reference thread walked -- is among the
+        reference's rows.
+    This pins the multi-photon-per-slot walk (each photon starting where the
+    previous one's draws ended) on the benchmark tissue itself."""
+    g = superset("five_layer")
+    T, Nref, seed = int(g["threads"]), int(g["photons"]), int(g["seed"])
+    q = -(-3 * Nref // (2 * T))
+    sim = load_case("five_layer")
+    sim.number_photons = q * T
+    matched = early = 0
+    with m.Simulation(sim, seed=seed, slots=T) as s:
+        s.run()
+        s.replay()
+        for sds in range(1, sim.num_sds + 1):
+            rows, _ = s.rows(sds)
+            ids, _ = s.detections(sds)
+            assert rows.shape[0] == ids.size
+            k = ids % q  # photon index within its slot (N = q*T: every slot has q)
+            ours = {r.tobytes(): int(kk) for r, kk in zip(rows, k)}
+            ref = g[f"rows_{sds}"]
+            refset = {r.tobytes() for r in ref}
+            missing = [i for i, r in enumerate(ref) if r.tobytes() not in ours]
+            assert not missing, f"SDS {sds}: reference rows {missing[:5]} not found"
+            matched += len(ref)
+            for r, kk in zip(rows, k):
+                if kk < Nref // (4 * T):
+                    assert r.tobytes() in refset, f"SDS {sds}: photon {kk} of its slot missing"
+                    early += 1
+    assert matched >= 50, f"only {matched} reference rows to compare"
+    assert early >= 5
+
+
+@pytest.mark.gpu
+def test_benchmark_tissue_reflectance_within_3_se_of_reference(gpu_available):
+    """The benchmark tissue at the reference's photon count with this
+    library's own slot layout (the benchmark's): per-SDS reflectance within 3
+    combined standard errors of the reference's output.txt."""
+    g = superset("five_layer")
+    Nref = int(g["photons"])
+    sim = load_case("five_layer")
+    sim.number_photons = Nref
+    with m.Simulation(sim, seed=int(g["seed"]) + 7) as s:
+        r = s.run()
+    ref_R = [float(v) for v in bytes(g["output_txt"]).decode().split()]
+    for i in range(sim.num_sds):
+        se = r.std_error[i] * np.sqrt(2.0)
+        assert abs(r.reflectance[i] - ref_R[i]) <= 3 * se + 1e-15, (i, r.reflectance[i], ref_R[i], se)

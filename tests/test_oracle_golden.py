@@ -19,11 +19,27 @@ at 1e-6 relative in fibre mode.
 import numpy as np
 import pytest
 
-from conftest import GOLDEN, load_case
+from conftest import CONFIGS, GOLDEN
 
 import oracle
 
+
+def load_case(case):
+    """The case's configuration read by the oracle's own reader (these tests
+    need no part of the CUDA library)."""
+    d = CONFIGS / case
+    return oracle.read_config(d / "sim_set.json", d / "input.txt")[0]
+
 CASES = ["fiber3", "ring5", "mismatch", "ringpt"]
+
+
+def close(a: float, b: float, tol: float) -> bool:
+    """|a - b| <= tol, or both NaN (the ring detector at pos = 0 of
+    example/HW8_A weighs its photons with acos of a division by zero,
+    transport.cu:915, which is NaN in the reference and here alike)."""
+    if np.isnan(a) or np.isnan(b):
+        return bool(np.isnan(a) and np.isnan(b))
+    return abs(a - b) <= tol
 
 
 def streams(g, S):
@@ -50,7 +66,7 @@ def test_oracle_replays_reference_photons(case, fp64):
         total = float(np.sum(ref[1:L + 1]))
         assert np.all(np.abs(row[1:L + 1] - ref[1:L + 1]) <= 1e-5 * total), (s, k)
         if ring:
-            assert abs(row[0] - ref[0]) <= 1e-2 * abs(ref[0]), (s, k, row[0], ref[0])
+            assert close(row[0], ref[0], 1e-2 * abs(ref[0])), (s, k, row[0], ref[0])
         elif fp64:
             assert abs(row[0] - ref[0]) <= 1e-6 * abs(ref[0]), (s, k, row[0], ref[0])
         else:
@@ -103,4 +119,4 @@ def test_oracle_statistics_match_reference_at_4x_threads(case):
         var = st.wsq[i] / N - mean * mean
         se = np.sqrt(max(var, 0.0) / (N - 1)) / 4294967295.0
         R = st.wsum[i] / scale
-        assert abs(R - ref_R[i]) <= 3 * np.sqrt(2.0) * se, (i, R, ref_R[i], se)
+        assert close(R, ref_R[i], 3 * np.sqrt(2.0) * se), (i, R, ref_R[i], se)

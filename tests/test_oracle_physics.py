@@ -6,9 +6,16 @@ by roulette; the only other change is the rounding of the float weight in
 `w - w_t`, tracked exactly.  In FP64 that rounding is zero."""
 import pytest
 
-from conftest import load_case
+from conftest import CONFIGS
 
 import oracle
+
+
+def load_case(case):
+    """The case's configuration read by the oracle's own reader (these tests
+    need no part of the CUDA library)."""
+    d = CONFIGS / case
+    return oracle.read_config(d / "sim_set.json", d / "input.txt")[0]
 
 
 def balance(e):
