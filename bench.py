@@ -546,7 +546,8 @@ def surrogate_arm(args) -> int:
     t0 = time.perf_counter()
     labels = sg.make_labels(base, n_baselines=args.baselines, photons=int(args.label_photons),
                             combos_per_baseline=args.combos // args.baselines, seed=1,
-                            mua_range=MUA_RANGE, mus_range=MUS_RANGE)
+                            mua_range=MUA_RANGE, mus_range=MUS_RANGE,
+                            mua_baseline=args.label_mua_baseline, mus_jitter=args.label_mus_jitter)
     label_s = time.perf_counter() - t0
     t0 = time.perf_counter()
     sur = sg.Surrogate.train(labels, epochs=args.epochs, batch=4096, lr=2e-3, seed=1,
@@ -629,7 +630,8 @@ def surrogate_arm(args) -> int:
                               "mc_rel_se_median": float(np.median(se)),
                               "heldout": args.heldout, "ref_photons": int(args.ref_photons)},
         "labels": {"count": int(labels.X.shape[0]), "baselines": args.baselines,
-                   "photons_per_baseline": int(args.label_photons), "seconds": label_s},
+                   "photons_per_baseline": int(args.label_photons), "seconds": label_s,
+                   "mua_baseline": args.label_mua_baseline, "mus_jitter": args.label_mus_jitter},
         "training": {"epochs": args.epochs, "seconds": train_s,
                      "final_loss": [float(v) for v in sur.history[-1]]},
         "config": {"workload": "surrogate: WMC labels, MLP 25->256x4->3 GELU, ensemble 4, "
@@ -833,6 +835,8 @@ def main() -> int:
     ap.add_argument("--max-photons", type=float, default=1e7)
     ap.add_argument("--baselines", type=int, default=512)
     ap.add_argument("--label-photons", type=float, default=2.5e6)
+    ap.add_argument("--label-mua-baseline", default="mid", choices=["mid", "low"])
+    ap.add_argument("--label-mus-jitter", type=float, default=0.05)
     ap.add_argument("--combos", type=int, default=2_000_000)
     ap.add_argument("--epochs", type=int, default=12)
     ap.add_argument("--queries", type=int, default=1_000_000)

@@ -178,19 +178,23 @@ class Labels:
 
 def make_labels(base: Sim, *, n_baselines: int, photons: int, combos_per_baseline: int,
                 mua_range=(0.05, 0.5), mus_range=(50.0, 250.0), mus_jitter: float = 0.05,
-                seed: int = 0, device: int = 0) -> Labels:
+                mua_baseline: str = "mid", seed: int = 0, device: int = 0) -> Labels:
     """White-MC labels: n_baselines tissues (mus drawn in mus_range, mua at
-    the middle of its range) walked with `photons` photons and replayed;
-    each replay relabelled to combos_per_baseline (mua', mus') with mua'
-    uniform in mua_range and mus' = mus * U(1 - mus_jitter, 1 + mus_jitter)
-    clipped to mus_range (so the training hull is the two ranges)."""
+    the middle of its range, or at its low end with mua_baseline="low")
+    walked with `photons` photons and replayed; each replay relabelled to
+    combos_per_baseline (mua', mus') with mua' uniform in mua_range and
+    mus' = mus * U(1 - mus_jitter, 1 + mus_jitter) clipped to mus_range (so
+    the training hull is the two ranges).  From the low end every mua'
+    rescale multiplies a photon's weight by exp(-dmua PL) <= 1, so long
+    paths never gain weight (no heavy-tailed rescale factors)."""
     rng = np.random.default_rng(seed)
     L, S = int(base.num_layers), int(base.num_sds)
     Xs, Ys, bl = [], [], []
     for b in range(n_baselines):
         sim = Sim.from_buffer_copy(base)
         sim.number_photons = photons
-        mua0 = np.full(L, 0.5 * (mua_range[0] + mua_range[1]))
+        mua0 = np.full(L, mua_range[0] if mua_baseline == "low"
+                       else 0.5 * (mua_range[0] + mua_range[1]))
         mus0 = rng.uniform(*mus_range, L)
         for l in range(L):
             sim.mua[l], sim.mus[l] = float(mua0[l]), float(mus0[l])
