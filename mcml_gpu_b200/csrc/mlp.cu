@@ -220,6 +220,12 @@ constexpr long long kTcSpin = 1ll << 22;
 // limit is far above the per-stage one and independent of it.
 constexpr long long kTcDrainSpin = 1ll << 26;
 
+// K columns per A chunk: the largest of 64, 32, 16 that divides K (K is a
+// multiple of 16), so that the chunks cover every column.
+__host__ __device__ __forceinline__ int tc_chunk_k(int K) {
+  return K % 64 == 0 ? 64 : K % 32 == 0 ? 32 : 16;
+}
+
 enum TcEpi {
   kTcBiasGelu = 0,  // H = bf16(gelu(acc + b)), Z = acc + b (optional)
   kTcBias = 1,      // Y = acc + b (FP32, the output layer)
@@ -406,8 +412,8 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1)
   const int slice = blockIdx.z % splits;  // K slice
   const int K = g.K, N = g.N;
   const int tiles = (g.M + TCM - 1) / TCM;
-  const int KC = K < 64 ? K : 64;  // K per chunk
-  const int nch = K / KC;          // 1..4 chunks per tile
+  const int KC = tc_chunk_k(K);   // K per chunk
+  const int nch = K / KC;          // chunks per tile
   const int nslots = g.slots;      // A ring: chunk i of the CTA's sequence uses slot i % nslots
   const uint32_t slot_bytes = (uint32_t)(KC / 8) * kLboA;
   const uint32_t lboB = (uint32_t)(N / 8) * 128;
@@ -740,10 +746,365 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Whole-network forward for inference on the tensor cores: every layer of
+// every member in one launch.  CTA (c, member z) takes batches of
+// batch_rows rows (whole 128-row tiles) and runs each batch through all the
+// layers before the next batch.  Per layer it loads that layer's weights
+// (the B operand, MN-major, no swizzle) and bias into shared memory, streams
+// the batch's activations in (layer 0: the normalised inputs by cp.async;
+// later layers: the CTA's own scratch rows by TMA, 128-byte swizzle) and
+// writes the layer's output back to its scratch (hidden layers: bias +
+// GELU, BF16, TMA stores) or to Y (the output layer: bias, FP32).  A CTA's
+// scratch (2 x batch_rows rows, ping-pong between layers) is read back by
+// the same CTA right after it was written, so the activations stay in L2
+// between layers instead of making an HBM round trip per layer, and one
+// launch replaces one per layer per chunk.  Roles, barriers and the
+// bounded waits are those of tc_layer_kernel; the barriers are set up
+// afresh for every (batch, layer) pass, after the previous pass drained.
+constexpr int kMaxFusedLayers = 12;
+
+struct FusedArgs {
+  int n;                // rows
+  int layers;           // weight matrices (depth + 1)
+  int ctas_per_member;  // gridDim.x
+  int batch_rows;       // rows per batch, a multiple of 128
+  int hidden;           // scratch row width (BF16 elements)
+  int K[kMaxFusedLayers], N[kMaxFusedLayers], n_valid[kMaxFusedLayers];
+  long long w_off[kMaxFusedLayers], b_off[kMaxFusedLayers];
+  const bf16 *X;        // n x K[0], normalised inputs shared by the members
+  const bf16 *W;        // BF16 parameters of member 0; member z at z * strideW
+  const float *Wf;      // FP32 parameters (the biases)
+  long long strideW;
+  float *Y;             // members x n x n_valid[last]
+  int slots;            // A ring slots
+  unsigned *status;
+  long long spin;
+};
+
+__global__ void __launch_bounds__(kTcWarps * 32, 1)
+    tc_fused_forward_kernel(const FusedArgs f, const __grid_constant__ CUtensorMap tmA,
+                            const __grid_constant__ CUtensorMap tmH) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char *smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int z = blockIdx.z;
+  const int nslots = f.slots;
+  const uint32_t slot_stride = 64 / 8 * kLboA;  // room for the widest chunk
+  // shared memory sized for the widest layer: B operand, A ring, staging,
+  // bias, barriers, TMEM slot
+  int maxKN = 0;
+  for (int l = 0; l < f.layers; ++l) maxKN = max(maxKN, f.K[l] * f.N[l]);
+  unsigned char *sB = smem;
+  unsigned char *sA = smem + (((size_t)maxKN * 2 + 1023) & ~(size_t)1023);
+  unsigned char *sStage = sA + (size_t)nslots * slot_stride;
+  float *sBias = reinterpret_cast<float *>(sStage + (size_t)8 * 2 * 2048);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(sBias + 256);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 37);
+  const uint32_t sA_u = smem_u32(sA), sB_u = smem_u32(sB), bars_u = smem_u32(bars);
+  auto a_full = [&](int s) { return bars_u + 8u * s; };
+  auto a_empty = [&](int s) { return bars_u + 8u * (16 + s); };
+  auto acc_full = [&](int b) { return bars_u + 8u * (32 + b); };
+  auto acc_empty = [&](int b) { return bars_u + 8u * (34 + b); };
+  const uint32_t drain_bar = bars_u + 8u * 36;
+
+  if (warp == 0) {  // two 256-column accumulators: all of tensor memory
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                     smem_u32(tslot)),
+                 "r"(512)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+  const int cta = z * gridDim.x + blockIdx.x;
+  const int BR = f.batch_rows;
+  const int batches = (f.n + BR - 1) / BR;
+  const bf16 *Wz = f.W + (long long)z * f.strideW;
+  const float *Wfz = f.Wf + (long long)z * f.strideW;
+  // a wait of this CTA timed out (written by the role, read after a barrier);
+  // beside the TMEM slot in the fixed part of the dynamic shared memory
+  volatile int &s_err = *reinterpret_cast<volatile int *>(tslot + 1);
+  if (tid == 0) s_err = 0;
+  bool inited = false;
+  bool failed = false;
+
+  for (int bt = blockIdx.x; bt < batches && !failed; bt += gridDim.x) {
+    const int r0 = bt * BR;                       // first row of the batch
+    const int rows = min(BR, f.n - r0);
+    const int tiles = (rows + TCM - 1) / TCM;
+    for (int l = 0; l < f.layers && !failed; ++l) {
+      const int K = f.K[l], N = f.N[l], nv = f.n_valid[l];
+      const bool last = l == f.layers - 1;
+      const int KC = tc_chunk_k(K);
+      const int nch = K / KC;
+      const uint32_t lboB = (uint32_t)(N / 8) * 128;
+      const bool tma = l > 0 && K % 64 == 0;
+      // scratch rows: input buffer (l-1)%2, output buffer l%2
+      const int a_row0 = (cta * 2 + ((l + 1) & 1)) * BR;
+      const int h_row0 = (cta * 2 + (l & 1)) * BR;
+      // ---- pass set-up: barriers afresh, this layer's weights and bias
+      __syncthreads();
+      if (tid == 0) {
+        // the previous pass completed every phase it started (no timeout,
+        // or the kernel would have stopped), so nothing arrives on these
+        if (inited) {
+          for (int c = 0; c < nslots; ++c) {
+            asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(a_full(c)) : "memory");
+            asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(a_empty(c)) : "memory");
+          }
+          for (int b = 0; b < 2; ++b) {
+            asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(acc_full(b)) : "memory");
+            asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(acc_empty(b)) : "memory");
+          }
+          asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(drain_bar) : "memory");
+        }
+        for (int c = 0; c < nslots; ++c) {
+          mbar_init(a_full(c), tma ? 1 : kProducers);
+          mbar_init(a_empty(c), 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+          mbar_init(acc_full(b), 1);
+          mbar_init(acc_empty(b), 256);
+        }
+        mbar_init(drain_bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+      }
+      inited = true;
+      const bf16 *W = Wz + f.w_off[l];
+      if (nv == N) {
+        const int nc8 = N / 8;
+        for (int c = tid; c < K * nc8; c += kTcWarps * 32) {
+          const int k_lo = c & 7, rest = c >> 3;
+          const int nc = rest % nc8, k = (rest / nc8) * 8 + k_lo;
+          const uint32_t dst = sB_u + (k >> 3) * lboB + nc * 128 + k_lo * 16;
+          const bf16 *src = W + (long long)k * N + nc * 8;
+          asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src)
+                       : "memory");
+        }
+      } else {
+        bf16 *sb = reinterpret_cast<bf16 *>(sB);
+        for (int e = tid; e < K * N; e += kTcWarps * 32) {
+          const int k = e / N, nn = e % N;
+          const bf16 v = nn < nv ? W[(long long)k * nv + nn] : __float2bfloat16(0.0f);
+          sb[((k >> 3) * lboB + (nn >> 3) * 128 + (k & 7) * 16 + (nn & 7) * 2) / 2] = v;
+        }
+      }
+      for (int c = tid; c < N; c += kTcWarps * 32) sBias[c] = c < nv ? Wfz[f.b_off[l] + c] : 0.0f;
+      asm volatile("cp.async.wait_all;\n" ::: "memory");
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+      __syncthreads();
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+      const uint32_t tmem = *tslot;
+
+      if (warp < 3 && tma) {
+        // ---- producer: this CTA's scratch rows of the layer's input
+        if (tid == 0) {
+          int gi = 0;
+          bool alive = true;
+          for (int t = 0; t < tiles && alive; ++t) {
+            for (int c = 0; c < nch; ++c, ++gi) {
+              const int slot = gi % nslots, use = gi / nslots;
+              if (use > 0 && !mbar_wait(a_empty(slot), (uint32_t)((use - 1) & 1), f.spin)) {
+                atomicOr(f.status, 1u);
+                s_err = 1;
+                alive = false;
+                break;
+              }
+              const uint32_t dst = sA_u + (uint32_t)slot * slot_stride;
+              const uint32_t bytes = (uint32_t)(KC / 8) * kLboA;
+              asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(
+                               a_full(slot)),
+                           "r"(bytes)
+                           : "memory");
+              asm volatile(
+                  "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+                  " [%0], [%1, {%3, %4, %5}], [%2];\n" ::"r"(dst),
+                  "l"(reinterpret_cast<uint64_t>(&tmA)), "r"(a_full(slot)), "r"(c * KC),
+                  "r"(a_row0 + t * TCM), "r"(0)
+                  : "memory");
+            }
+          }
+          for (int slot = 0; slot < nslots && slot < gi; ++slot) {
+            const int last_use = (gi - 1 - slot) / nslots;
+            if (!mbar_wait(a_full(slot), (uint32_t)(last_use & 1), kTcDrainSpin))
+              { atomicOr(f.status, 2u); s_err = 1; }
+          }
+        }
+        __syncwarp();
+      } else if (warp < 3) {
+        // ---- producers (layer 0): the normalised inputs by cp.async,
+        // rows past n as zeros
+        const int per_chunk = TCM * KC / 8;
+        int gi = 0;
+        for (int t = 0; t < tiles; ++t) {
+          const int m0 = r0 + t * TCM;
+          bool alive = true;
+          for (int c = 0; c < nch; ++c, ++gi) {
+            const int slot = gi % nslots, use = gi / nslots;
+            if (use > 0 && !mbar_wait(a_empty(slot), (uint32_t)((use - 1) & 1), f.spin)) {
+              atomicOr(f.status, 1u);
+                s_err = 1;
+              alive = false;
+              break;
+            }
+            const uint32_t base = sA_u + (uint32_t)slot * slot_stride;
+            for (int e = tid; e < per_chunk; e += kProducers) {
+              const int r_lo = e & 7, rest = e >> 3;
+              const int kl = rest % (KC / 8), r = (rest / (KC / 8)) * 8 + r_lo;
+              const uint32_t dst = base + kl * kLboA + (r >> 3) * 128 + r_lo * 16;
+              const int gr = m0 + r;
+              const bf16 *src = f.X + (long long)(gr < f.n ? gr : 0) * K + (c * (KC / 8) + kl) * 8;
+              const uint32_t bytes = gr < f.n ? 16u : 0u;
+              asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src),
+                           "r"(bytes)
+                           : "memory");
+            }
+            asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(
+                             a_full(slot))
+                         : "memory");
+          }
+          if (!alive) break;
+        }
+      } else if (warp == 3) {
+        // ---- MMA issuer
+        if (lane == 0) {
+          const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 16) |
+                                 ((uint32_t)(N >> 3) << 17) | ((uint32_t)(TCM >> 4) << 24);
+          for (int t = 0; t < tiles; ++t) {
+            const int b = t & 1, u = t >> 1;
+            if (u > 0 && !mbar_wait(acc_empty(b), (uint32_t)((u - 1) & 1), f.spin)) {
+              atomicOr(f.status, 1u);
+                s_err = 1;
+              break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            const uint32_t d = tmem + (uint32_t)(b * 256);
+            bool ok = true;
+            for (int c = 0; c < nch && ok; ++c) {
+              const int gi = t * nch + c, slot = gi % nslots, use = gi / nslots;
+              if (!mbar_wait(a_full(slot), (uint32_t)(use & 1), f.spin)) {
+                atomicOr(f.status, 1u);
+                s_err = 1;
+                ok = false;
+                break;
+              }
+              asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+              const uint32_t base = sA_u + (uint32_t)slot * slot_stride;
+              for (int j = 0; j < KC / 16; ++j) {
+                const int ks = c * (KC / 16) + j;
+                const uint64_t ad = tma ? umma_desc_sw128(base + 32 * j)
+                                        : umma_desc(base + 2 * j * kLboA, kLboA, 128);
+                const uint64_t bd = umma_desc(sB_u + 2 * ks * lboB, lboB, 128);
+                const uint32_t acc = ks > 0 ? 1u : 0u;
+                asm volatile(
+                    "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                    " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d),
+                    "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+                    : "memory");
+              }
+              umma_commit(a_empty(slot));
+            }
+            if (!ok) break;
+            umma_commit(acc_full(b));
+          }
+          umma_commit(drain_bar);
+          if (!mbar_wait(drain_bar, 0u, kTcDrainSpin)) { atomicOr(f.status, 2u); s_err = 1; }
+        }
+        __syncwarp();
+      } else {
+        // ---- epilogue: warp w drains TMEM lanes 32*(w%4).., column half (w-4)/4
+        const int q = warp & 3, half = (warp - 4) >> 2;
+        const int c_begin = half * (N / 2);
+        unsigned char *my_stage = sStage + (warp - 4) * 4096;
+        for (int t = 0; t < tiles; ++t) {
+          const int b = t & 1, u = t >> 1;
+          if (!__all_sync(0xffffffffu, mbar_wait(acc_full(b), (uint32_t)(u & 1), f.spin))) {
+            atomicOr(f.status, 1u);
+                s_err = 1;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+          const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * 256);
+          const int lrow = t * TCM + q * 32 + lane;  // row within the batch
+          if (!last) {
+            // bias + GELU -> BF16 staging -> TMA store into the scratch rows
+            TcArgs g{};
+            const int chunks = (N / 2) / 32;
+            auto emit = [&](const uint32_t (&v)[32], int c0, int buf) {
+              unsigned char *st = my_stage + buf * 2048;
+              if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 1;\n" ::: "memory");
+              __syncwarp();
+              epilogue32<kTcBiasGelu>(g, v, 0, 0, c0, sBias, st, lane);
+              asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+              __syncwarp();
+              if (lane == 0) {
+                asm volatile(
+                    "cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%2, %3, %4}], [%1];\n" ::"l"(
+                        reinterpret_cast<uint64_t>(&tmH)),
+                    "r"(smem_u32(st)), "r"(c0), "r"(h_row0 + t * TCM + q * 32), "r"(0)
+                    : "memory");
+                asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+              }
+            };
+            uint32_t va[32], vb[32];
+            tmem_ld32(va, tbase + c_begin);
+            tmem_wait();
+            for (int c = 0; c < chunks; c += 2) {
+              if (c + 1 < chunks) tmem_ld32(vb, tbase + c_begin + (c + 1) * 32);
+              emit(va, c_begin + c * 32, 0);
+              tmem_wait();
+              if (c + 1 < chunks) {
+                if (c + 2 < chunks) tmem_ld32(va, tbase + c_begin + (c + 2) * 32);
+                emit(vb, c_begin + (c + 1) * 32, 1);
+                tmem_wait();
+              }
+            }
+          } else {
+            // output layer: bias -> FP32 rows of Y (real columns, real rows)
+            const int grow = r0 + lrow;
+            for (int c0 = c_begin; c0 < c_begin + N / 2; c0 += 8) {
+              uint32_t v[8];
+              asm volatile(
+                  "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+                  : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+                    "=r"(v[6]), "=r"(v[7])
+                  : "r"(tbase + (uint32_t)c0));
+              tmem_wait();
+              if (lrow >= rows) continue;
+              float *y = f.Y + ((long long)z * f.n + grow) * nv;
+#pragma unroll
+              for (int i = 0; i < 8; ++i)
+                if (c0 + i < nv) y[c0 + i] = __uint_as_float(v[i]) + sBias[c0 + i];
+            }
+          }
+          asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+          mbar_arrive(acc_empty(b));
+        }
+      }
+      // ---- pass end: copies and stores complete before the next pass reads
+      // the scratch or reuses the ring, staging and barriers
+      asm volatile("cp.async.wait_all;\n" ::: "memory");
+      if (warp >= 4 && lane == 0) {
+        asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
+        asm volatile("fence.proxy.async.global;\n" ::: "memory");
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+      __syncthreads();
+      failed = s_err != 0;  // a timeout: stop after this drained pass
+    }
+  }
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(*tslot), "r"(512)
+                 : "memory");
+  }
+}
+
 constexpr size_t kTcSmemMax = 227 * 1024;  // opt-in shared memory per block
 constexpr size_t kTcSmemFixed = 256 * 4 + 37 * 8 + 16;  // bias, barriers, TMEM slot
 
-size_t tc_slot_bytes(int K) { return (size_t)(K < 64 ? K : 64) / 8 * kLboA; }
+size_t tc_slot_bytes(int K) { return (size_t)tc_chunk_k(K) / 8 * kLboA; }
 
 // A ring slots: as many as fit beside the weights (at most 16).
 size_t tc_align1k(size_t n) { return (n + 1023) & ~(size_t)1023; }
@@ -868,15 +1229,33 @@ cudaError_t tc_layer(const TcArgs &g, int members, cudaStream_t s) {
 }
 
 // X rows of a minibatch -> BF16, normalised, zero-padded to in_pad columns.
+// Training state read by the kernels of a step, so that one recorded step
+// (a CUDA graph) serves every minibatch of an epoch: the rows of the
+// epoch's shuffles consumed so far, the Adam steps taken, the learning rate.
+struct TrainStep {
+  unsigned long long offset;
+  long long t;
+  float lr;
+};
+
+// Marks a minibatch done: the next one starts `rows` further into the shuffles.
+__global__ void advance_step_kernel(TrainStep *st, unsigned long long rows) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->offset += rows;
+    st->t += 1;
+  }
+}
+
 __global__ void gather_x_kernel(const float *X, const uint32_t *idx, int n, int in_dim, int in_pad,
                                 const float *mean, const float *inv_std, long long idx_stride,
-                                bf16 *out, long long out_stride) {
+                                bf16 *out, long long out_stride, const TrainStep *st) {
   const int z = blockIdx.z;
   const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= (long long)n * in_pad) return;
   const int r = (int)(e / in_pad), c = (int)(e % in_pad);
   float v = 0.0f;
   if (c < in_dim) {
+    if (idx && st) idx += st->offset;
     const uint32_t row = idx ? idx[z * idx_stride + r] : (uint32_t)r;
     v = (X[(long long)row * in_dim + c] - mean[c]) * inv_std[c];
   }
@@ -887,10 +1266,11 @@ __global__ void gather_x_kernel(const float *X, const uint32_t *idx, int n, int 
 __global__ void loss_grad_kernel(const float *Yp, long long strideY, const float *T,
                                  const uint32_t *idx, long long idx_stride, int n, int out_dim,
                                  const float *tmean, const float *tinv, bf16 *dY,
-                                 long long strideD, float *loss) {
+                                 long long strideD, float *loss, const TrainStep *st) {
   const int z = blockIdx.z;
   const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   float l = 0.0f;
+  if (st) idx += st->offset;
   if (e < (long long)n * out_dim) {
     const int r = (int)(e / out_dim), c = (int)(e % out_dim);
     const uint32_t row = idx[z * idx_stride + r];
@@ -915,11 +1295,14 @@ __global__ void bias_grad_kernel(const bf16 *dZ, long long strideD, int n, int c
 }
 
 // Adam on the FP32 master weights; refreshes the BF16 mirror.
+// Adam step number st->t + 1 with learning rate st->lr.
 __global__ void adam_kernel(float *w, const float *grad, float *m, float *v, bf16 *w16,
-                            long long n, float lr, float b1, float b2, float eps, float c1,
-                            float c2) {
+                            long long n, const TrainStep *st, float b1, float b2, float eps) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  const float t = (float)(st->t + 1);
+  const float c1 = 1.0f - powf(b1, t), c2 = 1.0f - powf(b2, t);
+  const float lr = st->lr;
   const float gr = grad[i];
   const float mi = b1 * m[i] + (1.0f - b1) * gr;
   const float vi = b2 * v[i] + (1.0f - b2) * gr * gr;
@@ -995,6 +1378,12 @@ struct mcml_mlp {
   long long adam_t = 0;
   // activations for a batch of up to cap rows
   int cap = 0;
+  // whole-network inference (tc_fused_forward_kernel): inputs and outputs of
+  // up to fcap rows, and the CTAs' activation scratch
+  bf16 *d_fx = nullptr;            // fcap x in_pad
+  float *d_fy = nullptr;           // E x fcap x out
+  bf16 *d_act = nullptr;           // 2 x batch rows x hidden per CTA
+  long long fcap = 0;
   bf16 *d_x = nullptr;             // E x cap x in_pad
   float *d_z = nullptr;            // E x depth x cap x hidden (pre-activations)
   bf16 *d_h = nullptr;             // E x depth x cap x hidden (activations)
@@ -1004,6 +1393,16 @@ struct mcml_mlp {
   uint32_t *d_idx = nullptr;       // E x cap
   float *d_loss = nullptr;         // E
   uint32_t *d_perm = nullptr;      // E x n: one epoch's shuffles
+  TrainStep *d_step = nullptr;     // device-side minibatch offset, Adam step, learning rate
+  TrainStep h_step{};              // staging for its upload
+  // One recorded training step (a CUDA graph), replayed for every full
+  // minibatch of an epoch; recorded again when its inputs (X, T, n, batch,
+  // activation buffers) change.
+  cudaGraphExec_t step_exec = nullptr;
+  const float *step_X = nullptr, *step_T = nullptr;
+  uint64_t step_n = 0;
+  uint32_t step_batch = 0;
+  long long step_cap = 0;
   size_t perm_cap = 0;
 
   ~mcml_mlp() {
@@ -1016,6 +1415,11 @@ struct mcml_mlp {
     dfree(d_x); dfree(d_z); dfree(d_h); dfree(d_y); dfree(d_dy); dfree(d_dh); dfree(d_idx);
     dfree(d_loss);
     dfree(d_perm);
+    dfree(d_step);
+    dfree(d_fx);
+    dfree(d_fy);
+    dfree(d_act);
+    if (step_exec) cudaGraphExecDestroy(step_exec);
     dfree(d_status);
     if (own_stream && stream) cudaStreamDestroy(stream);
     if (prev >= 0 && prev != device) cudaSetDevice(prev);
@@ -1113,6 +1517,109 @@ int check_status(mcml_mlp *p) {
                                       "its issued copies and MMAs timed out");
     return set_error(MCML_E_BUDGET, "tensor-core kernel: a pipeline wait timed out "
                                     "(issued copies and MMAs drained)");
+  }
+  return MCML_OK;
+}
+
+// Whole-network inference (tc_fused_forward_kernel) applies when every
+// hidden layer can stream its activations by TMA and store them in 32-column
+// TMA tiles: hidden width a multiple of 64, at most kMaxFusedLayers layers,
+// an output of at most 16 columns.
+bool fused_eligible(const mcml_mlp *p) {
+  return p->hidden % 64 == 0 && p->hidden <= 256 && p->layers <= kMaxFusedLayers &&
+         p->out_dim <= 16 && p->in_pad <= 256;
+}
+
+constexpr int kFusedBatchRows = 512;          // rows a CTA takes through all layers at once
+constexpr long long kFusedRows = 1ll << 22;   // rows per launch
+
+// Tensor map over the activation scratch (hidden x rows BF16, one member
+// plane) with the given box and swizzle.
+bool encode_act_map(const mcml_mlp *p, long long rows, cuuint32_t bx, cuuint32_t by,
+                    CUtensorMapSwizzle sw, CUtensorMap *map) {
+  EncodeTiledFn fn = encode_tiled();
+  if (!fn) return false;
+  const cuuint64_t dims[3] = {(cuuint64_t)p->hidden, (cuuint64_t)rows, 1};
+  const cuuint64_t strides[2] = {(cuuint64_t)p->hidden * 2, (cuuint64_t)rows * p->hidden * 2};
+  const cuuint32_t box[3] = {bx, by, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, p->d_act, dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+int fused_predict(mcml_mlp *p, const float *X, uint64_t n, float *mean, float *spread) {
+  int dev = 0, sms = 0;
+  MLP_TRY(cudaGetDevice(&dev));
+  MLP_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const int per_member = std::max(1, sms / p->E);
+  const long long ctas = (long long)per_member * p->E;
+  const long long scratch_rows = ctas * 2 * kFusedBatchRows;
+  const long long rows_cap = std::min<long long>(kFusedRows, (long long)n);
+  if (!p->d_act) {
+    MLP_TRY(cudaMalloc(&p->d_act, scratch_rows * p->hidden * sizeof(bf16)));
+  }
+  if (rows_cap > p->fcap) {
+    dfree(p->d_fx);
+    dfree(p->d_fy);
+    p->fcap = 0;
+    MLP_TRY(cudaMalloc(&p->d_fx, rows_cap * p->in_pad * sizeof(bf16)));
+    MLP_TRY(cudaMalloc(&p->d_fy, p->E * rows_cap * p->out_dim * sizeof(float)));
+    p->fcap = rows_cap;
+  }
+  CUtensorMap amap, hmap;
+  std::memset(&amap, 0, sizeof(amap));
+  std::memset(&hmap, 0, sizeof(hmap));
+  if (!encode_act_map(p, scratch_rows, 64, TCM, CU_TENSOR_MAP_SWIZZLE_128B, &amap) ||
+      !encode_act_map(p, scratch_rows, 32, 32, CU_TENSOR_MAP_SWIZZLE_64B, &hmap))
+    return set_error(MCML_E_CUDA, "mlp: tensor maps of the activation scratch");
+  FusedArgs f;
+  std::memset(&f, 0, sizeof(f));
+  f.layers = p->layers;
+  f.ctas_per_member = per_member;
+  f.batch_rows = kFusedBatchRows;
+  f.hidden = p->hidden;
+  int maxKN = 0;
+  for (int l = 0; l < p->layers; ++l) {
+    f.K[l] = p->fan_in[l];
+    f.n_valid[l] = p->fan_out[l];
+    f.N[l] = (p->fan_out[l] + 15) / 16 * 16;
+    f.w_off[l] = p->w_off[l];
+    f.b_off[l] = p->b_off[l];
+    maxKN = std::max(maxKN, f.K[l] * f.N[l]);
+  }
+  f.W = p->d_w16;
+  f.Wf = p->d_w;
+  f.strideW = p->stride;
+  f.status = p->d_status;
+  f.spin = p->spin;
+  const size_t fixed = tc_align1k((size_t)maxKN * 2) + kTcStageBytes + kTcSmemFixed + 1024;
+  const size_t slot = tc_slot_bytes(64);
+  f.slots = (int)std::min<size_t>(16, (kTcSmemMax - fixed) / slot);
+  if (f.slots < 2) return set_error(MCML_E_INVALID, "mlp: layers too wide for the fused forward");
+  const size_t smem = fixed + (size_t)f.slots * slot;
+  static std::atomic<bool> configured[64];
+  if (dev >= 0 && dev < 64 && !configured[dev].load()) {
+    MLP_TRY(cudaFuncSetAttribute(tc_fused_forward_kernel,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmemMax));
+    configured[dev].store(true);
+  }
+  for (uint64_t r0 = 0; r0 < n; r0 += (uint64_t)rows_cap) {
+    const int rows = (int)std::min<uint64_t>((uint64_t)rows_cap, n - r0);
+    gather_x_kernel<<<dim3((unsigned)(((long long)rows * p->in_pad + 255) / 256), 1, 1), 256, 0,
+                      p->stream>>>(X + r0 * p->in_dim, nullptr, rows, p->in_dim, p->in_pad,
+                                   p->d_xmean, p->d_xinv, 0, p->d_fx, 0, nullptr);
+    MLP_TRY(cudaGetLastError());
+    f.n = rows;
+    f.X = p->d_fx;
+    f.Y = p->d_fy;
+    tc_fused_forward_kernel<<<dim3(per_member, 1, p->E), kTcWarps * 32, smem, p->stream>>>(f, amap,
+                                                                                        hmap);
+    MLP_TRY(cudaGetLastError());
+    ensemble_kernel<<<(unsigned)(((long long)rows * p->out_dim + 255) / 256), 256, 0, p->stream>>>(
+        p->d_fy, (long long)rows * p->out_dim, p->E, (long long)rows * p->out_dim, p->d_tmean,
+        p->d_tstd, p->out_dim, mean + r0 * p->out_dim, spread ? spread + r0 * p->out_dim : nullptr);
+    MLP_TRY(cudaGetLastError());
   }
   return MCML_OK;
 }
@@ -1287,6 +1794,7 @@ int mcml_mlp_create(const mcml_mlp_config *cfg, mcml_mlp **out) {
     MLP_TRY(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
     p->own_stream = true;
   }
+  MLP_TRY(cudaMalloc(&p->d_step, sizeof(TrainStep)));
   MLP_TRY(cudaMalloc(&p->d_w, total * sizeof(float)));
   MLP_TRY(cudaMalloc(&p->d_m, total * sizeof(float)));
   MLP_TRY(cudaMalloc(&p->d_v, total * sizeof(float)));
@@ -1400,14 +1908,15 @@ int mcml_mlp_gradients(mcml_mlp *p, const float *X, const float *T, int n, float
                           p->stream));
   const long long cap = p->cap;
   gather_x_kernel<<<dim3((unsigned)((n * p->in_pad + 255) / 256), 1, p->E), 256, 0, p->stream>>>(
-      X, p->d_idx, n, p->in_dim, p->in_pad, p->d_xmean, p->d_xinv, cap, p->d_x, cap * p->in_pad);
+      X, p->d_idx, n, p->in_dim, p->in_pad, p->d_xmean, p->d_xinv, cap, p->d_x, cap * p->in_pad,
+      nullptr);
   MLP_TRY(cudaGetLastError());
   rc = forward(p, n, true);
   if (rc) return rc;
   MLP_TRY(cudaMemsetAsync(p->d_loss, 0, p->E * sizeof(float), p->stream));
   loss_grad_kernel<<<dim3((unsigned)((n * p->out_dim + 255) / 256), 1, p->E), 256, 0, p->stream>>>(
       p->d_y, cap * p->out_dim, T, p->d_idx, cap, n, p->out_dim, p->d_tmean, p->d_tinv, p->d_dy,
-      cap * std::max(p->hidden, p->out_dim), p->d_loss);
+      cap * std::max(p->hidden, p->out_dim), p->d_loss, nullptr);
   MLP_TRY(cudaGetLastError());
   rc = backward(p, n);
   if (rc) return rc;
@@ -1432,9 +1941,8 @@ int mcml_mlp_train_epoch(mcml_mlp *p, const float *X, const float *T, uint64_t n
   MlpGuard gd(p->device);
   int rc = ensure_cap(p, (int)std::min<uint64_t>(batch, n));
   if (rc) return rc;
-  const long long cap = p->cap;
   // The epoch's shuffles (one per member) go to the device in one copy;
-  // minibatches index into them, so the loop below never waits for the host.
+  // minibatches index into them, so the steps below never wait for the host.
   std::vector<uint32_t> perm((size_t)p->E * n);
   for (int e = 0; e < p->E; ++e) {
     uint32_t *pe = &perm[(size_t)e * n];
@@ -1445,6 +1953,10 @@ int mcml_mlp_train_epoch(mcml_mlp *p, const float *X, const float *T, uint64_t n
   if (perm.size() > p->perm_cap) {
     dfree(p->d_perm);
     p->perm_cap = 0;
+    if (p->step_exec) {  // the recorded step reads the old shuffle buffer
+      cudaGraphExecDestroy(p->step_exec);
+      p->step_exec = nullptr;
+    }
     MLP_TRY(cudaMalloc(&p->d_perm, perm.size() * sizeof(uint32_t)));
     p->perm_cap = perm.size();
   }
@@ -1452,31 +1964,76 @@ int mcml_mlp_train_epoch(mcml_mlp *p, const float *X, const float *T, uint64_t n
                           cudaMemcpyHostToDevice, p->stream));
   // d_loss sums the minibatch means over the epoch
   MLP_TRY(cudaMemsetAsync(p->d_loss, 0, p->E * sizeof(float), p->stream));
-  uint64_t steps = 0;
-  const long long total = p->stride * p->E;
-  for (uint64_t b0 = 0; b0 + batch <= n || (b0 < n && steps == 0); b0 += batch) {
-    const int rows = (int)std::min<uint64_t>(batch, n - b0);
+  p->h_step.offset = 0;
+  p->h_step.t = p->adam_t;
+  p->h_step.lr = lr;
+  MLP_TRY(cudaMemcpyAsync(p->d_step, &p->h_step, sizeof(TrainStep), cudaMemcpyHostToDevice,
+                          p->stream));
+  // Full minibatches only (the rows left over wait for the next shuffle), or
+  // one step over all rows when there are fewer than a batch.
+  const int rows = (int)std::min<uint64_t>(batch, n);
+  const uint64_t steps = n >= batch ? n / batch : 1;
+  const long long cap = p->cap, total = p->stride * p->E;
+  // one step: gather, forward, loss, backward, Adam, advance
+  auto record_step = [&]() -> int {
     gather_x_kernel<<<dim3((unsigned)((rows * p->in_pad + 255) / 256), 1, p->E), 256, 0, p->stream>>>(
-        X, p->d_perm + b0, rows, p->in_dim, p->in_pad, p->d_xmean, p->d_xinv, (long long)n, p->d_x,
-        cap * p->in_pad);
+        X, p->d_perm, rows, p->in_dim, p->in_pad, p->d_xmean, p->d_xinv, (long long)n, p->d_x,
+        cap * p->in_pad, p->d_step);
     MLP_TRY(cudaGetLastError());
-    rc = forward(p, rows, true);
-    if (rc) return rc;
+    int r = forward(p, rows, true);
+    if (r) return r;
     loss_grad_kernel<<<dim3((unsigned)((rows * p->out_dim + 255) / 256), 1, p->E), 256, 0, p->stream>>>(
-        p->d_y, cap * p->out_dim, T, p->d_perm + b0, (long long)n, rows, p->out_dim, p->d_tmean,
-        p->d_tinv, p->d_dy, cap * std::max(p->hidden, p->out_dim), p->d_loss);
+        p->d_y, cap * p->out_dim, T, p->d_perm, (long long)n, rows, p->out_dim, p->d_tmean,
+        p->d_tinv, p->d_dy, cap * std::max(p->hidden, p->out_dim), p->d_loss, p->d_step);
     MLP_TRY(cudaGetLastError());
-    rc = backward(p, rows);
-    if (rc) return rc;
-    ++p->adam_t;
-    const float b1 = 0.9f, b2 = 0.999f;
-    const float c1 = 1.0f - std::pow(b1, (float)p->adam_t), c2 = 1.0f - std::pow(b2, (float)p->adam_t);
+    r = backward(p, rows);
+    if (r) return r;
     adam_kernel<<<(unsigned)((total + 255) / 256), 256, 0, p->stream>>>(
-        p->d_w, p->d_g, p->d_m, p->d_v, p->d_w16, total, lr, b1, b2, 1e-8f, c1, c2);
+        p->d_w, p->d_g, p->d_m, p->d_v, p->d_w16, total, p->d_step, 0.9f, 0.999f, 1e-8f);
     MLP_TRY(cudaGetLastError());
-    ++steps;
-    if (rows < (int)batch) break;
+    advance_step_kernel<<<1, 32, 0, p->stream>>>(p->d_step, (unsigned long long)rows);
+    MLP_TRY(cudaGetLastError());
+    return MCML_OK;
+  };
+  // The ~20 launches of a step are recorded once into a CUDA graph and the
+  // graph is replayed per minibatch: the launches are short and their
+  // host-side set-up dominated a step.  A stream that cannot be captured
+  // keeps the plain launches.
+  const bool same = p->step_exec && p->step_X == X && p->step_T == T && p->step_n == n &&
+                    p->step_batch == batch && p->step_cap == cap && steps > 1;
+  if (!same && p->step_exec) {
+    cudaGraphExecDestroy(p->step_exec);
+    p->step_exec = nullptr;
   }
+  if (!p->step_exec && steps > 1) {
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+      const int r = record_step();
+      const cudaError_t e = cudaStreamEndCapture(p->stream, &graph);
+      if (r == MCML_OK && e == cudaSuccess && graph &&
+          cudaGraphInstantiate(&p->step_exec, graph, 0) == cudaSuccess) {
+        p->step_X = X;
+        p->step_T = T;
+        p->step_n = n;
+        p->step_batch = batch;
+        p->step_cap = cap;
+      } else {
+        p->step_exec = nullptr;
+      }
+      if (graph) cudaGraphDestroy(graph);
+    }
+    cudaGetLastError();  // a failed capture leaves the plain launches below
+    clear_error();
+  }
+  for (uint64_t k = 0; k < steps; ++k) {
+    if (p->step_exec) {
+      MLP_TRY(cudaGraphLaunch(p->step_exec, p->stream));
+    } else {
+      rc = record_step();
+      if (rc) return rc;
+    }
+  }
+  p->adam_t += (long long)steps;
   std::vector<float> loss(p->E);
   MLP_TRY(cudaMemcpyAsync(loss.data(), p->d_loss, p->E * sizeof(float), cudaMemcpyDeviceToHost,
                           p->stream));
@@ -1488,12 +2045,17 @@ int mcml_mlp_train_epoch(mcml_mlp *p, const float *X, const float *T, uint64_t n
 }
 
 // Inference: X [n x in] DEVICE -> mean [n x out] and ensemble spread
-// [n x out] (DEVICE, de-normalised), in chunks of the activation buffers.
+// [n x out] (DEVICE, de-normalised).  Networks whose hidden width is a
+// multiple of 64 run all layers in one launch per up to 2^22 rows
+// (fused_predict); others, or MCML_MLP_LAYERWISE=1 in the environment, run
+// layer by layer in chunks of the activation buffers.
 int mcml_mlp_predict(mcml_mlp *p, const float *X, uint64_t n, float *mean, float *spread,
                      uint32_t chunk) {
   clear_error();
   if (!p || !X || !mean) return set_error(MCML_E_INVALID, "bad argument");
   MlpGuard gd(p->device);
+  const char *lw = std::getenv("MCML_MLP_LAYERWISE");
+  if (fused_eligible(p) && !(lw && lw[0] == '1')) return fused_predict(p, X, n, mean, spread);
   if (chunk == 0) chunk = 65536;
   int rc = ensure_cap(p, (int)std::min<uint64_t>(chunk, n));
   if (rc) return rc;
@@ -1502,7 +2064,7 @@ int mcml_mlp_predict(mcml_mlp *p, const float *X, uint64_t n, float *mean, float
     const int rows = (int)std::min<uint64_t>(cap, n - r0);
     gather_x_kernel<<<dim3((unsigned)((rows * p->in_pad + 255) / 256), 1, 1), 256, 0, p->stream>>>(
         X + r0 * p->in_dim, nullptr, rows, p->in_dim, p->in_pad, p->d_xmean, p->d_xinv, 0, p->d_x,
-        cap * p->in_pad);
+        cap * p->in_pad, nullptr);
     MLP_TRY(cudaGetLastError());
     rc = forward(p, rows, false, true);
     if (rc) return rc;
