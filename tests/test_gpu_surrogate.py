@@ -1,12 +1,14 @@
 """End to end: White-MC labels from replayed baselines -> MLP ensemble trained
 on the GPU -> served predictions, compared with plain MC.
 
+The network is configuration C3's: 25 inputs -> 4 hidden layers of 256,
+GELU -> 3 log-reflectances, an ensemble of 4, BF16 tensor-core training.
 The held-out tissues are drawn like the labels (a baseline's scattering
-within a few percent, clipped to 50-250 /cm, absorption anywhere in range).  The network must
-(a) agree with plain MC walked at 2e7 photons per tissue within 6 %
-median relative error (measured: 1.6 %, with the reference's own
-standard error at 0.4 %), and (b) beat plain MC given the same GPU time as
-the network's inference -- the gain the trained network brings over the
+within a few percent, clipped to 50-250 /cm, absorption anywhere in
+range).  The network must (a) agree with plain MC walked at 2e7 photons
+per tissue within 2 % median relative error (the references' own standard
+error is about 0.4 %), and (b) beat plain MC given the same GPU time as the
+network's inference -- the gain the trained network brings over the
 method without it.  Queries outside the training hull go to plain MC.
 """
 import time
@@ -42,9 +44,9 @@ def held_out(labels, count, rng, mua_range=(0.05, 0.5), jitter=0.05):
 @pytest.mark.gpu
 def test_surrogate_beats_equal_cost_plain_mc(gpu_available):
     base = base_sim()
-    labels = sg.make_labels(base, n_baselines=6, photons=3_000_000, combos_per_baseline=3000,
+    labels = sg.make_labels(base, n_baselines=8, photons=5_000_000, combos_per_baseline=4000,
                             seed=3)
-    sur = sg.Surrogate.train(labels, epochs=30, batch=1024, lr=2e-3, hidden=128, depth=3,
+    sur = sg.Surrogate.train(labels, epochs=40, batch=1024, lr=2e-3, hidden=256, depth=4,
                              ensemble=4, seed=1, max_spread=1.0)
     assert sur.history[-1].mean() < sur.history[0].mean()
     rng = np.random.default_rng(11)
@@ -80,7 +82,7 @@ def test_surrogate_beats_equal_cost_plain_mc(gpu_available):
     rel_cheap = np.abs(R_cheap - R_ref) / R_ref
     print("surrogate median rel err", np.median(rel), "MC SE/R", np.median(se / R_ref),
           "equal-cost MC photons", cheap_photons, "its median rel err", np.median(rel_cheap))
-    assert np.median(rel) < 0.06
+    assert np.median(rel) < 0.02
     assert np.median(rel) < np.median(rel_cheap)
     # out-of-hull queries fall back to plain MC
     far = m.Sim.from_buffer_copy(tissues[0])
