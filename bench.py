@@ -535,8 +535,10 @@ def surrogate_arm(args) -> int:
     """Surrogate training and serving: White-MC labels from replayed baselines of the 5-layer
     tissue (ring detectors at 0.5/1.0/1.5 cm, tests/golden/configs/surrogate),
     ensemble training on the GPU, serving of 1e6 queries (5 % outside the
-    training hull, whose answers come from plain MC at 1e7 photons), and the
-    error against plain MC on held-out tissues."""
+    training hull, whose answers come from plain MC at --fallback-photons),
+    and the error against plain MC at 1e8 photons on held-out tissues: the
+    network's answers inside the hull, the fallback's answers outside it, and
+    the two mixed in the proportions the queries have."""
     import torch
     import mcml_gpu_b200 as m
     import mcml_gpu_b200.surrogate as sg
@@ -550,8 +552,9 @@ def surrogate_arm(args) -> int:
                             mua_baseline=args.label_mua_baseline, mus_jitter=args.label_mus_jitter)
     label_s = time.perf_counter() - t0
     t0 = time.perf_counter()
+    fb_photons = int(args.fallback_photons)
     sur = sg.Surrogate.train(labels, epochs=args.epochs, batch=4096, lr=2e-3, seed=1,
-                             max_spread=0.05, fallback_photons=10_000_000)
+                             max_spread=0.05, fallback_photons=fb_photons)
     train_s = time.perf_counter() - t0
     rng = np.random.default_rng(5)
     # 1e6 queries: mua and mus of every layer uniform over the tissue's ranges;
@@ -579,14 +582,14 @@ def surrogate_arm(args) -> int:
     inside = np.all((X >= sur.lo - 1e-6) & (X <= sur.hi + 1e-6), axis=1)
     agree = np.all(spread.cpu().numpy() <= sur.max_spread, axis=1)
     fallback = ~(inside & agree)
-    # cost of the fallback: plain MC at 1e7 photons for a sample of flagged queries
-    fb_idx = np.nonzero(fallback)[0][:16]
+    # cost of the fallback: plain MC at fb_photons for a sample of flagged queries
+    fb_idx = np.nonzero(fallback)[0][:64]
     fb = []
     for i in fb_idx:
         s = m.Sim.from_buffer_copy(labels.baselines[0])
         for l in range(L):
             s.mua[l], s.mus[l] = float(X[i, 5 * l + 1]), float(X[i, 5 * l + 2])
-        s.number_photons = 10_000_000
+        s.number_photons = fb_photons
         fb.append(s)
     with m.Batch(fb, seed=3) as b:
         b.run()
@@ -611,6 +614,49 @@ def surrogate_arm(args) -> int:
     logR, _ = sur.predict(sg.features(held))
     rel = np.abs(np.exp(logR) - R_ref) / R_ref
     mc_evals = mc_rate / float(args.ref_photons)
+    # the fallback's own error: out-of-hull held-out tissues (one coefficient
+    # in the widened ranges' excess, like the flagged queries), plain MC at
+    # fb_photons against plain MC at ref_photons
+    out_t = []
+    for k in range(args.heldout_out):
+        s = m.Sim.from_buffer_copy(labels.baselines[0])
+        for l in range(L):
+            s.mua[l] = float(rng.uniform(*MUA_RANGE))
+            s.mus[l] = float(rng.uniform(*MUS_RANGE))
+        l, which = rng.integers(0, L), rng.integers(1, 3)
+        lo, hi = MUA_RANGE if which == 1 else MUS_RANGE
+        ext = 0.2 * (hi - lo)
+        v = rng.uniform(lo - ext, lo) if rng.random() < 0.5 else rng.uniform(hi, hi + ext)
+        if which == 1:
+            s.mua[l] = float(v)
+        else:
+            s.mus[l] = float(v)
+        out_t.append(s)
+    rel_fb = np.zeros((0, 3))
+    if out_t:
+        refs_o, fbs_o = [], []
+        for t in out_t:
+            a, b2 = m.Sim.from_buffer_copy(t), m.Sim.from_buffer_copy(t)
+            a.number_photons, b2.number_photons = int(args.ref_photons), fb_photons
+            refs_o.append(a)
+            fbs_o.append(b2)
+        with m.Batch(refs_o, seed=21) as b:
+            ro = b.run()
+        with m.Batch(fbs_o, seed=22) as b:
+            fo = b.run()
+        Ro = np.array([r.reflectance[:3] for r in ro])
+        Fo = np.array([r.reflectance[:3] for r in fo])
+        rel_fb = np.abs(Fo - Ro) / Ro
+    # served error: network answers and fallback answers in the queries' mix
+    frac_fb = float(fallback.mean())
+    vals = np.concatenate([rel.ravel(), rel_fb.ravel()])
+    wts = np.concatenate([np.full(rel.size, (1 - frac_fb) / max(rel.size, 1)),
+                          np.full(rel_fb.size, frac_fb / max(rel_fb.size, 1))])
+    order = np.argsort(vals)
+    cw = np.cumsum(wts[order]) / wts.sum()
+
+    def wq(q):
+        return float(vals[order][np.searchsorted(cw, q)])
     ref_evals, ref_note = reference_plain_mc_evals(cfg, held[:2], int(args.ref_photons))
     print(json.dumps({
         "metric": "SDS-reflectance evals/s", "impl": "mcml-surrogate",
@@ -622,13 +668,25 @@ def surrogate_arm(args) -> int:
         "speedup_vs_plain_mc_inside_hull": (nq / mlp_s) / mc_evals,
         "reference_plain_mc_evals_per_s": ref_evals, "reference_plain_mc_run": ref_note,
         "speedup_vs_reference_plain_mc": (nq / serve_s) / ref_evals if ref_evals else None,
-        "fallback_fraction": float(fallback.mean()),
-        "fallback_s_per_query_at_1e7": fb_per_query_s,
+        "fallback_fraction": frac_fb,
+        "fallback_photons": fb_photons,
+        "fallback_s_per_query": fb_per_query_s,
+        "speedup_cap_from_fallback": float(args.ref_photons) / max(frac_fb * fb_photons, 1.0),
         "error_vs_plain_mc": {"median_rel": float(np.median(rel)),
                               "p90_rel": float(np.percentile(rel, 90)),
                               "per_sds_median": [float(v) for v in np.median(rel, axis=0)],
+                              "per_sds_p90": [float(v) for v in np.percentile(rel, 90, axis=0)],
                               "mc_rel_se_median": float(np.median(se)),
-                              "heldout": args.heldout, "ref_photons": int(args.ref_photons)},
+                              "heldout": args.heldout, "ref_photons": int(args.ref_photons),
+                              "note": "network answers, held-out tissues inside the hull"},
+        "fallback_error_vs_plain_mc": {
+            "median_rel": float(np.median(rel_fb)) if rel_fb.size else None,
+            "p90_rel": float(np.percentile(rel_fb, 90)) if rel_fb.size else None,
+            "heldout": len(out_t),
+            "note": "plain MC at fallback_photons on out-of-hull held-out tissues"},
+        "served_error_vs_plain_mc": {"median_rel": wq(0.5), "p90_rel": wq(0.9),
+                                     "note": "network and fallback answers weighted by the "
+                                             "queries' fallback fraction"},
         "labels": {"count": int(labels.X.shape[0]), "baselines": args.baselines,
                    "photons_per_baseline": int(args.label_photons), "seconds": label_s,
                    "mua_baseline": args.label_mua_baseline, "mus_jitter": args.label_mus_jitter},
@@ -841,6 +899,9 @@ def main() -> int:
     ap.add_argument("--epochs", type=int, default=12)
     ap.add_argument("--queries", type=int, default=1_000_000)
     ap.add_argument("--heldout", type=int, default=1000)
+    ap.add_argument("--heldout-out", type=int, default=40,
+                    help="out-of-hull held-out tissues for the fallback's error")
+    ap.add_argument("--fallback-photons", type=float, default=2e6)
     ap.add_argument("--ref-photons", type=float, default=1e8)
     args = ap.parse_args()
     if args.impl == "reference":
