@@ -200,18 +200,19 @@ def test_pipeline_wait_timeout_is_reported_and_drained(gpu_available, monkeypatc
 @pytest.mark.gpu
 @pytest.mark.parametrize("hidden,depth,n", [(256, 4, 3000), (64, 3, 1000), (128, 2, 70000)])
 def test_fused_forward_equals_layer_by_layer(hidden, depth, n, gpu_available, monkeypatch):
-    """With a hidden width that is a multiple of 64, predict() runs every
-    layer of every member in one launch (the fused kernel, activations kept
-    in each CTA's L2-resident scratch); MCML_MLP_LAYERWISE=1 forces one
-    launch per layer.  Both round to BF16 at the same points and issue the
-    same tensor-core MMAs in the same order, so they agree bit for bit --
+    """With a hidden width that is a multiple of 64 and MCML_MLP_FUSED=1,
+    predict() runs every layer of every member in one launch (the fused
+    kernel, activations kept in each CTA's L2-resident scratch); without it,
+    one launch per layer.  Both round to BF16 at the same points and issue
+    the same tensor-core MMAs in the same order, so they agree bit for bit --
     including a last batch of rows that is not a whole 512-row batch."""
     rng = np.random.default_rng(13)
     X = torch.from_numpy(rng.normal(size=(n, 25)).astype(np.float32)).cuda()
     mlp = sg.MLP(25, 3, hidden=hidden, depth=depth, ensemble=4, seed=21)
     mlp.set_normalization(np.zeros(25), np.ones(25), np.zeros(3), np.ones(3))
+    monkeypatch.setenv("MCML_MLP_FUSED", "1")
     fm, fs = mlp.predict(X)
-    monkeypatch.setenv("MCML_MLP_LAYERWISE", "1")
+    monkeypatch.setenv("MCML_MLP_FUSED", "0")
     lm, ls = mlp.predict(X)
     assert torch.equal(fm, lm), float((fm - lm).abs().max())
     assert torch.equal(fs, ls)
