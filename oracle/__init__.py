@@ -52,7 +52,7 @@ def load() -> C.CDLL:
     lib.oracle_walk_stream.argtypes = [vp, C.c_int, vp, C.c_uint64, vp, vp, vp, vp]
     lib.oracle_walk_stream.restype = C.c_int
     lib.oracle_replay_stream.argtypes = [vp, C.c_int, C.c_int, vp, C.c_uint64, vp, vp, vp, vp,
-                                         vp]
+                                         vp, vp]
     lib.oracle_replay_stream.restype = C.c_int
     lib.oracle_run.argtypes = [vp, C.c_int, C.c_uint64, C.c_uint64, C.c_uint64, C.c_int,
                                C.POINTER(Stats), vp, vp, vp, C.c_uint64, vp]
@@ -91,8 +91,9 @@ def walk_stream(sim, u: np.ndarray, fp64: bool = False):
 
 def replay_stream(sim, sds: int, u: np.ndarray, fp64: bool = False, grid=None):
     """Replay of one photon for 1-based sds on recorded uniforms.
-    Returns (row[L+2] float64, interactions[L], A_rz or None, A0_z or None, used)
-    or None if the draws ran out."""
+    Returns (row[L+2] float64, interactions[L], A_rz or None, A0_z or None,
+    used, w_exit) or None if the draws ran out; w_exit is the photon's weight
+    as it leaves through the detector (before a ring detector weighs it)."""
     u = np.ascontiguousarray(u, dtype=np.float32)
     L = sim.num_layers
     row = np.zeros(L + 2, dtype=np.float64)
@@ -103,11 +104,12 @@ def replay_stream(sim, sds: int, u: np.ndarray, fp64: bool = False, grid=None):
         arz = np.zeros((nz, nr), dtype=np.uint64)
         a0z = np.zeros(nz, dtype=np.uint64)
     used = C.c_uint64(0)
+    w_exit = C.c_double(0.0)
     rc = load().oracle_replay_stream(C.byref(sim), int(fp64), sds, _p(u), u.size, _p(row),
-                                     _p(inter), _p(arz), _p(a0z), C.byref(used))
+                                     _p(inter), _p(arz), _p(a0z), C.byref(used), C.byref(w_exit))
     if rc != 0:
         return None
-    return row, inter, arz, a0z, int(used.value)
+    return row, inter, arz, a0z, int(used.value), float(w_exit.value)
 
 
 def run(sim, n: int, seed: int, *, first: int = 0, fp64: bool = False, threads: int = 0,

@@ -494,7 +494,7 @@ struct Grid {
 // counts.  Returns false if the draws ran out.
 template <typename R, typename Rng>
 bool walk_replay(Rng &g, const Tab<R> &t, int sds, double *row, uint32_t *inter,
-                 const Grid &grid) {
+                 const Grid &grid, double *w_exit = nullptr) {
   const int L = t.n_layers;
   Ph<R> p;
   launch(p, g, t);
@@ -520,6 +520,7 @@ bool walk_replay(Rng &g, const Tab<R> &t, int sds, double *row, uint32_t *inter,
           R wd;
           if (det_hit(p, t, sds, wd)) {
             w_det = wd;
+            if (w_exit) *w_exit = (double)p.w;  // the weight the detector weighs
             break;
           }
           if (uni<R>(g) > t.det_refl) break;
@@ -599,9 +600,11 @@ int oracle_walk_stream(const mcml_sim *sim, int fp64, const float *u, uint64_t n
 
 // Replay of one photon for SDS sds (1-based) driven by recorded uniforms.
 // row[L+2], inter[L]; A_rz (nz*nr) / A0_z (nz) of this SDS may be null.
+// w_exit (may be NULL): the photon's weight as it leaves through the
+// detector, before the ring weighting (transport.cu:1000-1002).
 int oracle_replay_stream(const mcml_sim *sim, int fp64, int sds, const float *u, uint64_t n_u,
                          double *row, uint32_t *inter, uint64_t *A_rz, uint64_t *A0_z,
-                         uint64_t *used) {
+                         uint64_t *used, double *w_exit) {
   StreamRng g{u, n_u};
   Grid grid;
   grid.A_rz = A_rz;
@@ -610,11 +613,11 @@ int oracle_replay_stream(const mcml_sim *sim, int fp64, int sds, const float *u,
   if (fp64) {
     Tab<double> t;
     make_tab(*sim, t);
-    ok = walk_replay(g, t, sds, row, inter, grid);
+    ok = walk_replay(g, t, sds, row, inter, grid, w_exit);
   } else {
     Tab<float> t;
     make_tab(*sim, t);
-    ok = walk_replay(g, t, sds, row, inter, grid);
+    ok = walk_replay(g, t, sds, row, inter, grid, w_exit);
   }
   if (used) *used = g.i;
   return ok ? 0 : -1;

@@ -29,8 +29,9 @@ from conftest import GOLDEN, load_case
 import mcml_gpu_b200 as m
 
 GOLDEN_DIR = Path(os.environ.get("MCML_GOLDEN_DIR", GOLDEN))
-CASES = ["fiber3", "ring5", "mismatch", "ringpt", "three_layer"]
-STAT_CASES = ["fiber3", "ring5", "mismatch", "ringpt"]
+CASES = ["fiber3", "ring5", "mismatch", "ringpt", "three_layer", "surrogate", "hw8a",
+         "head_model"]
+STAT_CASES = ["fiber3", "ring5", "mismatch", "ringpt", "surrogate", "hw8a", "head_model"]
 
 
 def same_or_both_nan(a: float, b: float, tol: float) -> bool:

@@ -9,10 +9,16 @@ CPU with exactly those draws must reproduce the reference's rows:
     float, the same float operations);
   * per-layer pathlengths within 1e-5 of the photon's total pathlength
     (libm logf/sinf/... stand in for the GPU's __logf/__sincosf/...);
-  * in ring mode the weight within 1e-2 relative: the ring weight is
-    w*acos(t)/pi, and for exits near a ring edge t is near 1, where acos
-    has an unbounded derivative and magnifies last-bit differences of the
-    exit position (observed up to 1.4e-3).
+  * in ring mode the weight within 1e-2 relative (observed up to 4.4e-3):
+    the ring weight is w*acos(t)/pi with t = (d^2 + pos^2 - r^2)/(2 d pos)
+    from the exit position, and acos magnifies the exit position's last-bit
+    differences as t nears 1.  Where 1 - t is itself of the order of float
+    resolution -- the 0.001 cm ring at 0.8 cm of example/head_model, where
+    1 - t <= r^2/(2 pos^2) = 8e-7 -- the weight is ill-conditioned (10 %
+    apart for one photon), so the detector cosine t is compared instead,
+    within 1e-6 (it agrees to one float ulp).  t is recovered from each
+    weight as cos(pi * w_det / w) with the photon's exit weight w from the
+    oracle, equal to the reference's (the fibre weights match exactly).
 The FP64 oracle meets the same bounds except that its weights are compared
 at 1e-6 relative in fibre mode.
 """
@@ -30,7 +36,7 @@ def load_case(case):
     d = CONFIGS / case
     return oracle.read_config(d / "sim_set.json", d / "input.txt")[0]
 
-CASES = ["fiber3", "ring5", "mismatch", "ringpt"]
+CASES = ["fiber3", "ring5", "mismatch", "ringpt", "surrogate", "hw8a", "head_model"]
 
 
 def close(a: float, b: float, tol: float) -> bool:
@@ -66,13 +72,20 @@ def test_oracle_replays_reference_photons(case, fp64):
         total = float(np.sum(ref[1:L + 1]))
         assert np.all(np.abs(row[1:L + 1] - ref[1:L + 1]) <= 1e-5 * total), (s, k)
         if ring:
-            assert close(row[0], ref[0], 1e-2 * abs(ref[0])), (s, k, row[0], ref[0])
+            w_exit = got[5]
+            if np.isnan(ref[0]) or np.isnan(row[0]):
+                assert np.isnan(ref[0]) and np.isnan(row[0]), (s, k, row[0], ref[0])
+            elif abs(row[0] - ref[0]) > 1e-2 * abs(ref[0]):
+                t_ours = np.cos(np.pi * row[0] / w_exit)
+                t_ref = np.cos(np.pi * float(ref[0]) / w_exit)
+                assert abs(t_ours - t_ref) <= 1e-6, (s, k, row[0], ref[0], t_ours, t_ref)
         elif fp64:
             assert abs(row[0] - ref[0]) <= 1e-6 * abs(ref[0]), (s, k, row[0], ref[0])
         else:
             assert np.float32(row[0]) == ref[0], (s, k, row[0], ref[0])
         n += 1
-    assert n >= sim.num_sds
+    # every SDS the reference detected photons at is checked
+    assert n >= sum(1 for s in range(1, sim.num_sds + 1) if g[f"rows_{s}"].shape[0] > 0)
 
 
 @pytest.mark.parametrize("case", CASES)
