@@ -33,6 +33,7 @@
 
 #include "../../include/mcml_b200.h"
 #include "internal.h"
+#include "kernels.h"
 #include "params.h"
 #include "photon.cuh"
 
@@ -103,7 +104,8 @@ __global__ void batch_seed_kernel(const BatchSet *sets, const uint64_t *prefix, 
   }
 }
 
-template <int kBlock, int kMinBlocks, bool kSrcOblique, bool kDetOblique>
+// kGlass: some set has a tissue layer with mutr == FLT_MAX (see walk_step).
+template <int kBlock, int kMinBlocks, bool kSrcOblique, bool kDetOblique, bool kGlass>
 __global__ void __launch_bounds__(kBlock, kMinBlocks) batch_walk_kernel(const BatchArgs A) {
   curandStateXORWOW st;
   st.boxmuller_flag = 0;
@@ -151,7 +153,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) batch_walk_kernel(const Ba
   launch_photon<kSrcOblique>(p, &st, *tp, start_w);
   for (;;) {
     const int base = b * 32;
-    const bool alive = walk_step<kDetOblique>(p, st, *tp, n_layers, n_sds, det_refl,
+    const bool alive = walk_step<kDetOblique, kGlass>(p, st, *tp, n_layers, n_sds, det_refl,
                                               [&](int i, float w) {
                                                 atomicAdd(&A.det_count[base + i], 1ull);
                                                 atomicAdd(&A.wsum[base + i], (double)w);
@@ -174,16 +176,20 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) batch_walk_kernel(const Ba
 
 struct Variant {
   int block, min_blocks;
-  const void *fn[4];
+  const void *fn[8];  // [glass*4 + src_oblique*2 + det_oblique]
 };
 
 template <int B, int M>
 Variant make_variant() {
   return Variant{B, M,
-                 {(const void *)batch_walk_kernel<B, M, false, false>,
-                  (const void *)batch_walk_kernel<B, M, false, true>,
-                  (const void *)batch_walk_kernel<B, M, true, false>,
-                  (const void *)batch_walk_kernel<B, M, true, true>}};
+                 {(const void *)batch_walk_kernel<B, M, false, false, false>,
+                  (const void *)batch_walk_kernel<B, M, false, true, false>,
+                  (const void *)batch_walk_kernel<B, M, true, false, false>,
+                  (const void *)batch_walk_kernel<B, M, true, true, false>,
+                  (const void *)batch_walk_kernel<B, M, false, false, true>,
+                  (const void *)batch_walk_kernel<B, M, false, true, true>,
+                  (const void *)batch_walk_kernel<B, M, true, false, true>,
+                  (const void *)batch_walk_kernel<B, M, true, true, true>}};
 }
 
 const std::vector<Variant> &variants() {
@@ -216,7 +222,7 @@ struct mcml_batch {
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   int B = 0;
-  int variant_kind = 0;  // src_oblique*2 + det_oblique
+  int variant_kind = 0;  // glass*4 + src_oblique*2 + det_oblique
   std::vector<mcml_sim> sims;
   std::vector<DevParams> params;
   std::vector<BatchSet> sets;
@@ -462,6 +468,7 @@ int mcml_batch_create(const mcml_sim *sims, int num_sets, const mcml_batch_opts 
     const int rc = derive(&sims[i], &der);
     if (rc) return rc;
     fill_dev_params(sims[i], der, sims[i].number_photons, 1, b->params[i]);
+    if (has_glass_layer(b->params[i])) b->variant_kind |= 4;
     BatchSet &s = b->sets[i];
     s.num_photons = sims[i].number_photons;
     s.seed = o.seed + (uint64_t)i;

@@ -408,12 +408,13 @@ int choose_walk(mcml_ctx *c) {
   const int block = c->opts.block_size ? (int)c->opts.block_size : 128;
   int minb = c->opts.blocks_per_sm ? (int)c->opts.blocks_per_sm : (block == 128 ? 8 : 2048 / block / 2);
   const bool so = c->sim.source_probe_oblique != 0, dobl = c->sim.detector_probe_oblique != 0;
-  const void *fn = walk_kernel_ptr(block, minb, so, dobl);
+  const bool glass = has_glass_layer(c->P);
+  const void *fn = walk_kernel_ptr(block, minb, so, dobl, glass);
   bool limit = false;  // no variant capped for minb: run the uncapped one, minb blocks/SM
   if (!fn) {
     limit = c->opts.blocks_per_sm != 0;
     minb = 1;
-    fn = walk_kernel_ptr(block, 1, so, dobl);
+    fn = walk_kernel_ptr(block, 1, so, dobl, glass);
   }
   if (!fn) return set_error(MCML_E_INVALID, "block_size must be 64, 128 or 256");
   DeviceGuard g(c->device);

@@ -18,6 +18,7 @@
 //   * Detections are appended to one global record buffer; the replay
 //     re-walks each record from its saved XORWOW state, again with
 //     per-lane dynamic work fetching.
+#include <cfloat>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -126,7 +127,8 @@ __global__ void seed_slots_kernel(uint64_t seed, uint64_t slot_begin, uint64_t n
 
 // ---------------------------------------------------------------------------
 // First pass (MCd, transport.cu:341-471).
-template <int kBlock, int kMinBlocks, bool kSrcOblique, bool kDetOblique>
+// kGlass: some tissue layer has mutr == FLT_MAX (see walk_step).
+template <int kBlock, int kMinBlocks, bool kSrcOblique, bool kDetOblique, bool kGlass>
 __global__ void __launch_bounds__(kBlock, kMinBlocks)
     walk_kernel(const __grid_constant__ DevParams P, const WalkArgs A) {
   __shared__ SmemTables t;
@@ -164,7 +166,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks)
   launch_photon<kSrcOblique>(p, &st, t, P.start_weight);
 
   for (;;) {
-    const bool alive = walk_step<kDetOblique>(
+    const bool alive = walk_step<kDetOblique, kGlass>(
         p, st, t, (int)P.n_layers, (int)P.n_sds, P.det_reflectance,
         [&](int i, float w) { append_record(A, photon_index(), i, w, sc); });
     if (!alive) {
@@ -390,17 +392,21 @@ cudaError_t launch_seed_slots(uint64_t seed, uint64_t slot_begin, uint64_t num_s
 // second number caps the registers per thread (65536 / (threads * blocks)).
 struct WalkVariant {
   int block, min_blocks;
-  const void *fn[4];  // [src_oblique*2 + det_oblique]
+  const void *fn[8];  // [glass*4 + src_oblique*2 + det_oblique]
 };
 
 template <int B, int M>
 static WalkVariant make_variant() {
   return WalkVariant{B,
                      M,
-                     {(const void *)walk_kernel<B, M, false, false>,
-                      (const void *)walk_kernel<B, M, false, true>,
-                      (const void *)walk_kernel<B, M, true, false>,
-                      (const void *)walk_kernel<B, M, true, true>}};
+                     {(const void *)walk_kernel<B, M, false, false, false>,
+                      (const void *)walk_kernel<B, M, false, true, false>,
+                      (const void *)walk_kernel<B, M, true, false, false>,
+                      (const void *)walk_kernel<B, M, true, true, false>,
+                      (const void *)walk_kernel<B, M, false, false, true>,
+                      (const void *)walk_kernel<B, M, false, true, true>,
+                      (const void *)walk_kernel<B, M, true, false, true>,
+                      (const void *)walk_kernel<B, M, true, true, true>}};
 }
 
 static const WalkVariant *walk_variants(int *n) {
@@ -413,18 +419,24 @@ static const WalkVariant *walk_variants(int *n) {
   return v;
 }
 
-const void *walk_kernel_ptr(int block, int min_blocks, bool src_obl, bool det_obl) {
+const void *walk_kernel_ptr(int block, int min_blocks, bool src_obl, bool det_obl, bool glass) {
   int n = 0;
   const WalkVariant *v = walk_variants(&n);
   for (int i = 0; i < n; ++i)
     if (v[i].block == block && v[i].min_blocks == min_blocks)
-      return v[i].fn[(src_obl ? 2 : 0) + (det_obl ? 1 : 0)];
+      return v[i].fn[(glass ? 4 : 0) + (src_obl ? 2 : 0) + (det_obl ? 1 : 0)];
   return nullptr;
+}
+
+bool has_glass_layer(const DevParams &P) {
+  for (uint32_t l = 1; l <= P.n_layers; ++l)
+    if (P.mutr[l] == FLT_MAX) return true;
+  return false;
 }
 
 cudaError_t launch_walk(const DevParams &P, const WalkArgs &A, bool src_obl, bool det_obl,
                         int block, int min_blocks, int grid, cudaStream_t stream) {
-  const void *fn = walk_kernel_ptr(block, min_blocks, src_obl, det_obl);
+  const void *fn = walk_kernel_ptr(block, min_blocks, src_obl, det_obl, has_glass_layer(P));
   if (!fn) return cudaErrorInvalidValue;
   void *args[] = {(void *)&P, (void *)&A};
   return cudaLaunchKernel(fn, dim3(grid), dim3(block), args, 0, stream);

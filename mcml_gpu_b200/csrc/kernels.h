@@ -47,7 +47,10 @@ cudaError_t launch_seed_slots(uint64_t seed, uint64_t slot_begin, uint64_t num_s
                               int sm_count, cudaStream_t stream);
 cudaError_t launch_walk(const DevParams &P, const WalkArgs &A, bool src_obl, bool det_obl,
                         int block, int min_blocks, int grid, cudaStream_t stream);
-const void *walk_kernel_ptr(int block, int min_blocks, bool src_obl, bool det_obl);
+// The walk kernel of a launch shape; glass: some tissue layer has
+// mutr == FLT_MAX (has_glass_layer), which needs the conditional draw.
+const void *walk_kernel_ptr(int block, int min_blocks, bool src_obl, bool det_obl, bool glass);
+bool has_glass_layer(const DevParams &P);
 cudaError_t launch_replay(const DevParams &P, const ReplayArgs &A, bool src_obl, bool det_obl,
                           bool ref_grid, int grid, cudaStream_t stream);
 // The first D records -- and, when rows is not null, their replay rows

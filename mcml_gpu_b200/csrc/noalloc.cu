@@ -32,6 +32,7 @@
 
 #include "../../include/mcml_b200.h"
 #include "internal.h"
+#include "kernels.h"
 #include "params.h"
 #include "photon.cuh"
 
@@ -83,7 +84,7 @@ __device__ __forceinline__ void tally(Header *h, int sds, float w) {
 
 // The first pass (walk_step) with detections summed per SDS in place of
 // appended records.
-template <bool kSrcOblique, bool kDetOblique>
+template <bool kSrcOblique, bool kDetOblique, bool kGlass>
 __global__ void __launch_bounds__(128) noalloc_walk_kernel(const __grid_constant__ DevParams P,
                                                            unsigned char *scratch) {
   __shared__ SmemTables t;
@@ -122,7 +123,7 @@ __global__ void __launch_bounds__(128) noalloc_walk_kernel(const __grid_constant
   if (!next_slot()) return;
   launch_photon<kSrcOblique>(p, &st, t, P.start_weight);
   for (;;) {
-    const bool alive = walk_step<kDetOblique>(p, st, t, n_layers, n_sds, P.det_reflectance,
+    const bool alive = walk_step<kDetOblique, kGlass>(p, st, t, n_layers, n_sds, P.det_reflectance,
                                               [&](int i, float w) { tally(h, i, w); });
     if (!alive) {
       steps_acc += (uint32_t)p.steps;
@@ -160,7 +161,7 @@ struct DeviceSetup {
   bool done = false;
   unsigned long long ctx_id = 0;  // context the address belongs to (0: unknown)
   unsigned char *scratch = nullptr;
-  int grid[4] = {0, 0, 0, 0};
+  int grid[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 };
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
@@ -197,12 +198,17 @@ unsigned long long current_context_id() {
   return id;
 }
 
+// variant: glass*4 + src_oblique*2 + det_oblique
 const void *walk_fn(int variant) {
   switch (variant) {
-    case 0: return (const void *)noalloc_walk_kernel<false, false>;
-    case 1: return (const void *)noalloc_walk_kernel<false, true>;
-    case 2: return (const void *)noalloc_walk_kernel<true, false>;
-    default: return (const void *)noalloc_walk_kernel<true, true>;
+    case 0: return (const void *)noalloc_walk_kernel<false, false, false>;
+    case 1: return (const void *)noalloc_walk_kernel<false, true, false>;
+    case 2: return (const void *)noalloc_walk_kernel<true, false, false>;
+    case 3: return (const void *)noalloc_walk_kernel<true, true, false>;
+    case 4: return (const void *)noalloc_walk_kernel<false, false, true>;
+    case 5: return (const void *)noalloc_walk_kernel<false, true, true>;
+    case 6: return (const void *)noalloc_walk_kernel<true, false, true>;
+    default: return (const void *)noalloc_walk_kernel<true, true, true>;
   }
 }
 
@@ -222,7 +228,7 @@ int setup_device(int device, DeviceSetup **out) {
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     if (e != cudaSuccess)
       return set_error(MCML_E_CUDA, std::string("cudaDeviceGetAttribute: ") + cudaGetErrorString(e));
-    for (int v = 0; v < 4; ++v) {
+    for (int v = 0; v < 8; ++v) {
       int nb = 0;
       e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, walk_fn(v), 128, 0);
       if (e != cudaSuccess)
@@ -278,7 +284,8 @@ extern "C" int mcml_run_noalloc(const mcml_sim *sim, uint64_t seed, uint64_t slo
     DevParams P;
     fill_dev_params(*sim, der, N, S, P);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    const int variant = (sim->source_probe_oblique ? 2 : 0) + (sim->detector_probe_oblique ? 1 : 0);
+    const int variant = (has_glass_layer(P) ? 4 : 0) + (sim->source_probe_oblique ? 2 : 0) +
+                        (sim->detector_probe_oblique ? 1 : 0);
     noalloc_seed_kernel<<<(unsigned)((S + 255) / 256), 256, 0, s>>>(d->scratch, seed, S);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) {
