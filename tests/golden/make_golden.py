@@ -20,7 +20,9 @@ reference's own random numbers.  A second, nondeterministic run at 4x the
 thread count gives the statistical fixture.  The reference's summary.json
 of each run is stored too, for the drop-in test of the command line.
 
-Superset fixtures (``--superset five_layer:1000000000``): the reference
+Superset fixtures (``--superset five_layer:1000000000,three_layer:10000000000``,
+configs 1 and 0 of the benchmark, whose narrow fibres need that many
+photons for detections): the reference
 at N well above its thread count T, where each thread walks about N/T
 photons and the split between threads depends on timing, but each
 thread's sequence of photons does not.  The fixture keeps every
@@ -57,7 +59,7 @@ import mcml_gpu_b200 as mcml  # noqa: E402
 SEED = 20261203
 PARITY_CASES = ["fiber3", "ring5", "mismatch", "ringpt", "three_layer", "surrogate", "hw8a",
                 "head_model"]
-SUPERSET_CASES = "five_layer:1000000000"
+SUPERSET_CASES = "five_layer:1000000000,three_layer:10000000000"
 STREAM_PHOTONS_PER_SDS = 6
 
 

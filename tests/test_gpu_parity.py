@@ -206,10 +206,15 @@ def superset(case):
     return np.load(p)
 
 
+SUPERSET_CASES = ["five_layer"]
+
+
 @pytest.mark.gpu
-def test_benchmark_tissue_rows_of_reference_found_bit_exact(gpu_available):
-    """The 5-layer benchmark tissue (config 1), its three oblique fibres, at
-    1e9 photons.  The reference walked them on T threads (about N/T photons
+@pytest.mark.parametrize("case", SUPERSET_CASES)
+def test_benchmark_tissue_rows_of_reference_found_bit_exact(case, gpu_available):
+    """The benchmark tissues with their three oblique fibres: config 1 (5
+    layers, g = 0.9) at 1e9 photons, config 0 (3 layers, g = 0) at 1e10.
+    The reference walked them on T threads (about N/T photons
     each; which thread takes the last photons depends on timing, but each
     thread's sequence of photons -- subsequence t, one photon after another
     -- does not).  This library walks the same T subsequences with 1.5 N/T
@@ -221,10 +226,10 @@ def test_benchmark_tissue_rows_of_reference_found_bit_exact(gpu_available):
         reference's rows.
     This pins the multi-photon-per-slot walk (each photon starting where the
     previous one's draws ended) on the benchmark tissue itself."""
-    g = superset("five_layer")
+    g = superset(case)
     T, Nref, seed = int(g["threads"]), int(g["photons"]), int(g["seed"])
     q = -(-3 * Nref // (2 * T))
-    sim = load_case("five_layer")
+    sim = load_case(case)
     sim.number_photons = q * T
     matched = early = 0
     with m.Simulation(sim, seed=seed, slots=T) as s:
@@ -250,13 +255,14 @@ def test_benchmark_tissue_rows_of_reference_found_bit_exact(gpu_available):
 
 
 @pytest.mark.gpu
-def test_benchmark_tissue_reflectance_within_3_se_of_reference(gpu_available):
+@pytest.mark.parametrize("case", SUPERSET_CASES)
+def test_benchmark_tissue_reflectance_within_3_se_of_reference(case, gpu_available):
     """The benchmark tissue at the reference's photon count with this
     library's own slot layout (the benchmark's): per-SDS reflectance within 3
     combined standard errors of the reference's output.txt."""
-    g = superset("five_layer")
+    g = superset(case)
     Nref = int(g["photons"])
-    sim = load_case("five_layer")
+    sim = load_case(case)
     sim.number_photons = Nref
     with m.Simulation(sim, seed=int(g["seed"]) + 7) as s:
         r = s.run()
