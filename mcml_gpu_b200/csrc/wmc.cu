@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(kThreads, 4) wmc_kernel(const float *F, uint64
                                                        const float *coef, uint64_t C,
                                                        double inv_scale, double *out) {
   static_assert(K % 2 == 0, "K = 2L+2 is even");
-  __shared__ __align__(16) float2 sF[kChunk / 2][K];  // [photon pair][k]
+  __shared__ __align__(16) float2 sF[2][kChunk / 2][K];  // [buffer][photon pair][k]
   const uint64_t c0 = ((uint64_t)blockIdx.x * kThreads + threadIdx.x) * kPer;
   float2 a[kPer][K];
 #pragma unroll
@@ -99,20 +99,46 @@ __global__ void __launch_bounds__(kThreads, 4) wmc_kernel(const float *F, uint64
   const uint64_t per = (chunks + gridDim.y - 1) / gridDim.y;
   const uint64_t d0 = blockIdx.y * per * kChunk;
   const uint64_t d1 = d0 + per * kChunk < D ? d0 + per * kChunk : D;
-  for (uint64_t base = d0; base < d1; base += kChunk) {
+  // Chunk staging, double-buffered: the next chunk's features travel
+  // (4-byte cp.async each) while this one is contracted.  Photons past the
+  // end (padding to whole pairs of pairs) get weight 0: log2 w = -inf
+  // (k = K-2) and 0 elsewhere, so their exp2 term is 0.
+  auto stage = [&](uint64_t base, int buf) {
     const int n = (int)((d1 - base) < (uint64_t)kChunk ? (d1 - base) : (uint64_t)kChunk);
-    const int np = (n + 3) / 4 * 2;  // photon pairs, an even number (padding below)
-    __syncthreads();
+    const int np = (n + 3) / 4 * 2;
     for (int idx = threadIdx.x; idx < np * K; idx += kThreads) {
       const int jp = idx / K, k = idx % K;
       const int j = 2 * jp;
-      // photons past n (padding to whole pairs of pairs) have weight 0:
-      // log2 w = -inf (k = K-2) and 0 elsewhere, so their exp2 term is 0
+      float *dst = reinterpret_cast<float *>(&sF[buf][jp][k]);
       const float pad = k == K - 2 ? -INFINITY : 0.0f;
-      const float f0 = j < n ? F[(base + j) * kMaxK + k] : pad;
-      const float f1 = j + 1 < n ? F[(base + j + 1) * kMaxK + k] : pad;
-      sF[jp][k] = make_float2(f0, f1);
+      if (j < n)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(
+                         (unsigned)__cvta_generic_to_shared(dst)),
+                     "l"(F + (base + j) * kMaxK + k)
+                     : "memory");
+      else
+        dst[0] = pad;
+      if (j + 1 < n)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(
+                         (unsigned)__cvta_generic_to_shared(dst + 1)),
+                     "l"(F + (base + j + 1) * kMaxK + k)
+                     : "memory");
+      else
+        dst[1] = pad;
     }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+  int cur = 0;
+  if (d0 < d1) stage(d0, 0);
+  for (uint64_t base = d0; base < d1; base += kChunk) {
+    const int n = (int)((d1 - base) < (uint64_t)kChunk ? (d1 - base) : (uint64_t)kChunk);
+    const int np = (n + 3) / 4 * 2;  // photon pairs, an even number
+    const bool more = base + kChunk < d1;
+    if (more) stage(base + kChunk, cur ^ 1);
+    if (more)
+      asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+    else
+      asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
     float2 acc[kPer];
 #pragma unroll
@@ -127,7 +153,7 @@ __global__ void __launch_bounds__(kThreads, 4) wmc_kernel(const float *F, uint64
       for (int k = 0; k < K; k += 2) {
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
-          const float4 f = *reinterpret_cast<const float4 *>(&sF[jp + h][k]);
+          const float4 f = *reinterpret_cast<const float4 *>(&sF[cur][jp + h][k]);
 #pragma unroll
           for (int r = 0; r < kPer; ++r)
             e[h][r] = __ffma2_rn(a[r][k], make_float2(f.x, f.y), e[h][r]);
@@ -144,6 +170,8 @@ __global__ void __launch_bounds__(kThreads, 4) wmc_kernel(const float *F, uint64
     }
 #pragma unroll
     for (int r = 0; r < kPer; ++r) total[r] += (double)acc[r].x + (double)acc[r].y;
+    __syncthreads();  // all warps are done with this buffer before it is refilled
+    cur ^= 1;
   }
 #pragma unroll
   for (int r = 0; r < kPer; ++r)
@@ -178,8 +206,15 @@ cudaError_t launch_wmc(const float *F, uint64_t D, const float *coef, uint64_t C
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  // one wave: as many blocks as are resident at once (every block gets the
+  // same number of photon chunks, so a second wave would only add a tail)
+  int resident = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, wmc_kernel<K>, kThreads, 0) !=
+          cudaSuccess ||
+      resident < 1)
+    resident = 4;
   const uint64_t chunks = (D + kChunk - 1) / kChunk;
-  const uint64_t want = ((uint64_t)4 * sms + gx - 1) / gx;
+  const uint64_t want = ((uint64_t)resident * sms + gx - 1) / gx;
   const unsigned gy = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(std::min<uint64_t>(chunks, want), 65535));
   cudaError_t e = cudaMemsetAsync(out, 0, C * sizeof(double), s);
   if (e != cudaSuccess) return e;

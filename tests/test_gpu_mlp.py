@@ -128,7 +128,8 @@ def cpu_forward(params, shapes, X, xm, xs, tm, ts):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("hidden,depth,n", [(256, 4, 300), (64, 3, 129), (128, 2, 1000)])
+@pytest.mark.parametrize("hidden,depth,n", [(256, 4, 300), (64, 3, 129), (128, 2, 1000),
+                                            (64, 2, 70000)])  # 70000: several tiles per CTA
 def test_tensor_core_forward_matches_cpu_reference(hidden, depth, n, gpu_available):
     """predict() runs the tcgen05 forward: ensemble mean and spread against
     a float64 CPU forward that rounds to bf16 where the kernel does (GEMM
@@ -214,5 +215,14 @@ def test_fused_forward_equals_layer_by_layer(hidden, depth, n, gpu_available, mo
     fm, fs = mlp.predict(X)
     monkeypatch.setenv("MCML_MLP_FUSED", "0")
     lm, ls = mlp.predict(X)
+    # both against the float64 CPU forward first, so a failure says which path is off
+    Xn = X.cpu().numpy()
+    z = np.zeros(25)
+    ys = np.stack([cpu_forward(mlp.params(e), mlp.layer_shapes(), Xn, z, np.ones(25),
+                               np.zeros(3), np.ones(3)) for e in range(4)])
+    scale = float(np.abs(ys).mean())
+    err_f = float(np.max(np.abs(fm.cpu().numpy() - ys.mean(0))))
+    err_l = float(np.max(np.abs(lm.cpu().numpy() - ys.mean(0))))
+    assert err_f < 1e-2 * scale and err_l < 1e-2 * scale, (err_f, err_l, scale)
     assert torch.equal(fm, lm), float((fm - lm).abs().max())
     assert torch.equal(fs, ls)

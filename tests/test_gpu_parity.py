@@ -206,7 +206,7 @@ def superset(case):
     return np.load(p)
 
 
-SUPERSET_CASES = ["five_layer"]
+SUPERSET_CASES = ["five_layer", "three_layer"]
 
 
 @pytest.mark.gpu
