@@ -448,14 +448,16 @@ def wmc_arm(args) -> int:
     D = rows.shape[0]
     terms = D * C / (ms / 1e3)
     K = 2 * L + 2
-    # per term: K FMAs issued as K/2 paired FMAs (two photons each), one MUFU
-    # exp2, half a paired add and K/2 16-byte shared loads shared by the
-    # 2 photons x 2 combos of a thread = `ops` issue slots; the FP32 lanes
-    # still do K + 1 operations (a paired instruction saves an issue slot,
-    # not a lane).  Bound per SM and clock: min(128 / ops issue,
-    # 128 / (K + 1) FP32 lanes, 16 MUFU).
-    ops = K / 2 + 1 + 0.5 + K / 8
-    lanes = K + 1
+    # per term: the exponent starts at log2 w and takes 2L FMAs, issued as L
+    # paired FMAs (two photons each), then one MUFU exp2 and half a paired
+    # add; the 16-byte shared loads (K-2 per 8 terms, plus two 8-byte loads
+    # of log2 w) are shared by the 2 photons x 2 combos of a thread.  That
+    # is `ops` issue slots; the FP32 lanes still do 2L + 1 operations (a
+    # paired instruction saves an issue slot, not a lane: it holds the
+    # lanes for two cycles).  Bound per SM and clock: min(128 / ops issue,
+    # 128 / (2L + 1) FP32 lanes, 16 MUFU).
+    ops = L + 1 + 0.5 + K / 8
+    lanes = 2 * L + 1
     f_sm = clocks.get("sm_mhz") or 1965.0
     per_clk = {"issue": 128.0 / ops, "fp32": 128.0 / lanes, "mufu": 16.0}
     bound = min(per_clk, key=per_clk.get)
@@ -892,11 +894,11 @@ def main() -> int:
     ap.add_argument("--min-photons", type=float, default=1e5)
     ap.add_argument("--max-photons", type=float, default=1e7)
     ap.add_argument("--baselines", type=int, default=512)
-    ap.add_argument("--label-photons", type=float, default=2.5e6)
-    ap.add_argument("--label-mua-baseline", default="mid", choices=["mid", "low"])
+    ap.add_argument("--label-photons", type=float, default=1e7)
+    ap.add_argument("--label-mua-baseline", default="low", choices=["mid", "low"])
     ap.add_argument("--label-mus-jitter", type=float, default=0.05)
     ap.add_argument("--combos", type=int, default=2_000_000)
-    ap.add_argument("--epochs", type=int, default=12)
+    ap.add_argument("--epochs", type=int, default=20)
     ap.add_argument("--queries", type=int, default=1_000_000)
     ap.add_argument("--heldout", type=int, default=1000)
     ap.add_argument("--heldout-out", type=int, default=40,

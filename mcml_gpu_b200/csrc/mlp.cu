@@ -787,26 +787,14 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1)
 // the batch's activations in (layer 0: the normalised inputs by cp.async;
 // later layers: the CTA's own scratch rows by TMA, 128-byte swizzle) and
 // writes the layer's output back to its scratch (hidden layers: bias +
-// GELU, BF16) or to Y (the output layer: bias, FP32).  A CTA's scratch
-// (2 x batch_rows rows, ping-pong between layers) is read back by the same
-// CTA right after it was written, so the activations stay in L2 between
-// layers, and one launch replaces one per layer per chunk.
-//
-// Roles (20 warps): warps 0-2 produce A (layer 0: all 96 threads by
-// cp.async; later layers: warp 0, lane 0, by TMA), warp 3 lane 0 issues the
-// MMAs into two 256-column tensor-memory accumulators, and 16 epilogue
-// warps drain them: warp w reads the TMEM lanes 32*(w%4).. (the rows it may
-// access) and a quarter of the columns, (w-4)/4, so four warps share each
-// row quarter and the bias/GELU work of a tile is spread over four warps
-// per scheduler.  The epilogue stores each row's BF16 activations straight
-// to the scratch (two 16-byte stores per 16 columns); a proxy fence before
-// the pass-end barrier orders those generic stores before the next layer's
-// TMA reads.  The barriers are set up afresh for every (batch, layer) pass,
-// after the previous pass drained; every wait is bounded.
+// GELU, BF16, TMA stores) or to Y (the output layer: bias, FP32).  A CTA's
+// scratch (2 x batch_rows rows, ping-pong between layers) is read back by
+// the same CTA right after it was written, so the activations stay in L2
+// between layers instead of making an HBM round trip per layer, and one
+// launch replaces one per layer per chunk.  Roles, barriers and the
+// bounded waits are those of tc_layer_kernel; the barriers are set up
+// afresh for every (batch, layer) pass, after the previous pass drained.
 constexpr int kMaxFusedLayers = 12;
-constexpr int kFusedWarps = 20;
-constexpr int kFusedThreads = kFusedWarps * 32;
-constexpr int kFusedEpiThreads = 16 * 32;
 
 struct FusedArgs {
   int n;                // rows
@@ -821,60 +809,28 @@ struct FusedArgs {
   const float *Wf;      // FP32 parameters (the biases)
   long long strideW;
   float *Y;             // members x n x n_valid[last]
-  bf16 *act;            // activation scratch, rows x hidden (the tensor map's)
   int slots;            // A ring slots
   unsigned *status;
   long long spin;
 };
 
-__device__ __forceinline__ void tmem_ld16(uint32_t (&v)[16], uint32_t taddr) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
-      "%14,%15}, [%16];\n"
-      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
-        "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
-        "=r"(v[14]), "=r"(v[15])
-      : "r"(taddr));
-}
-
-__device__ __forceinline__ void tmem_ld4(uint32_t (&v)[4], uint32_t taddr) {
-  asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];\n"
-               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3])
-               : "r"(taddr));
-}
-
-// Bias + GELU of 16 accumulator columns [c0, c0+16) of one row, stored as
-// BF16 at dst (32 bytes, 16-byte aligned).
-__device__ __forceinline__ void fused_gelu16(const uint32_t (&v)[16], const float *sBias, int c0,
-                                             bf16 *dst) {
-  __align__(16) __nv_bfloat162 h[8];
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const float2 b = *reinterpret_cast<const float2 *>(sBias + c0 + 2 * i);
-    const float2 g2 = gelu2(
-        __fadd2_rn(make_float2(__uint_as_float(v[2 * i]), __uint_as_float(v[2 * i + 1])), b));
-    h[i] = __floats2bfloat162_rn(g2.x, g2.y);
-  }
-  uint4 *d = reinterpret_cast<uint4 *>(dst);
-  d[0] = reinterpret_cast<const uint4 *>(h)[0];
-  d[1] = reinterpret_cast<const uint4 *>(h)[1];
-}
-
-__global__ void __launch_bounds__(kFusedThreads, 1)
-    tc_fused_forward_kernel(const FusedArgs f, const __grid_constant__ CUtensorMap tmA) {
+__global__ void __launch_bounds__(kTcWarps * 32, 1)
+    tc_fused_forward_kernel(const FusedArgs f, const __grid_constant__ CUtensorMap tmA,
+                            const __grid_constant__ CUtensorMap tmH) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char *smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int z = blockIdx.z;
   const int nslots = f.slots;
   const uint32_t slot_stride = 64 / 8 * kLboA;  // room for the widest chunk
-  // shared memory sized for the widest layer: B operand, A ring, bias,
-  // barriers, TMEM slot
+  // shared memory sized for the widest layer: B operand, A ring, staging,
+  // bias, barriers, TMEM slot
   int maxKN = 0;
   for (int l = 0; l < f.layers; ++l) maxKN = max(maxKN, f.K[l] * f.N[l]);
   unsigned char *sB = smem;
   unsigned char *sA = smem + (((size_t)maxKN * 2 + 1023) & ~(size_t)1023);
-  float *sBias = reinterpret_cast<float *>(sA + (size_t)nslots * slot_stride);
+  unsigned char *sStage = sA + (size_t)nslots * slot_stride;
+  float *sBias = reinterpret_cast<float *>(sStage + (size_t)8 * 2 * 2048);
   uint64_t *bars = reinterpret_cast<uint64_t *>(sBias + 256);
   uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 37);
   const uint32_t sA_u = smem_u32(sA), sB_u = smem_u32(sB), bars_u = smem_u32(bars);
@@ -939,7 +895,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
         }
         for (int b = 0; b < 2; ++b) {
           mbar_init(acc_full(b), 1);
-          mbar_init(acc_empty(b), kFusedEpiThreads);
+          mbar_init(acc_empty(b), 256);
         }
         mbar_init(drain_bar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
@@ -948,7 +904,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
       const bf16 *W = Wz + f.w_off[l];
       if (nv == N) {
         const int nc8 = N / 8;
-        for (int c = tid; c < K * nc8; c += kFusedThreads) {
+        for (int c = tid; c < K * nc8; c += kTcWarps * 32) {
           const int k_lo = c & 7, rest = c >> 3;
           const int nc = rest % nc8, k = (rest / nc8) * 8 + k_lo;
           const uint32_t dst = sB_u + (k >> 3) * lboB + nc * 128 + k_lo * 16;
@@ -958,13 +914,13 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
         }
       } else {
         bf16 *sb = reinterpret_cast<bf16 *>(sB);
-        for (int e = tid; e < K * N; e += kFusedThreads) {
+        for (int e = tid; e < K * N; e += kTcWarps * 32) {
           const int k = e / N, nn = e % N;
           const bf16 v = nn < nv ? W[(long long)k * nv + nn] : __float2bfloat16(0.0f);
           sb[((k >> 3) * lboB + (nn >> 3) * 128 + (k & 7) * 16 + (nn & 7) * 2) / 2] = v;
         }
       }
-      for (int c = tid; c < N; c += kFusedThreads) sBias[c] = c < nv ? Wfz[f.b_off[l] + c] : 0.0f;
+      for (int c = tid; c < N; c += kTcWarps * 32) sBias[c] = c < nv ? Wfz[f.b_off[l] + c] : 0.0f;
       asm volatile("cp.async.wait_all;\n" ::: "memory");
       asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
       asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
@@ -1002,10 +958,8 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
           }
           for (int slot = 0; slot < nslots && slot < gi; ++slot) {
             const int last_use = (gi - 1 - slot) / nslots;
-            if (!mbar_wait(a_full(slot), (uint32_t)(last_use & 1), kTcDrainSpin)) {
-              atomicOr(f.status, 2u);
-              s_err = 1;
-            }
+            if (!mbar_wait(a_full(slot), (uint32_t)(last_use & 1), kTcDrainSpin))
+              { atomicOr(f.status, 2u); s_err = 1; }
           }
         }
         __syncwarp();
@@ -1021,7 +975,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
             const int slot = gi % nslots, use = gi / nslots;
             if (use > 0 && !mbar_wait(a_empty(slot), (uint32_t)((use - 1) & 1), f.spin)) {
               atomicOr(f.status, 1u);
-              s_err = 1;
+                s_err = 1;
               alive = false;
               break;
             }
@@ -1052,7 +1006,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
             const int b = t & 1, u = t >> 1;
             if (u > 0 && !mbar_wait(acc_empty(b), (uint32_t)((u - 1) & 1), f.spin)) {
               atomicOr(f.status, 1u);
-              s_err = 1;
+                s_err = 1;
               break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
@@ -1086,55 +1040,74 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
             umma_commit(acc_full(b));
           }
           umma_commit(drain_bar);
-          if (!mbar_wait(drain_bar, 0u, kTcDrainSpin)) {
-            atomicOr(f.status, 2u);
-            s_err = 1;
-          }
+          if (!mbar_wait(drain_bar, 0u, kTcDrainSpin)) { atomicOr(f.status, 2u); s_err = 1; }
         }
         __syncwarp();
       } else {
-        // ---- epilogue: warp w drains TMEM lanes 32*(w%4).., columns
-        // [part*N/4, (part+1)*N/4) with part = (w-4)/4
-        const int q = warp & 3, part = (warp - 4) >> 2;
-        const int cpp = N / 4;  // columns per part: a multiple of 16 (hidden) or 4 (output)
-        const int c_begin = part * cpp;
+        // ---- epilogue: warp w drains TMEM lanes 32*(w%4).., column half (w-4)/4
+        const int q = warp & 3, half = (warp - 4) >> 2;
+        const int c_begin = half * (N / 2);
+        unsigned char *my_stage = sStage + (warp - 4) * 4096;
+        int sbuf = 0;  // staging tile of the next store, alternating as in tc_layer_kernel
         for (int t = 0; t < tiles; ++t) {
           const int b = t & 1, u = t >> 1;
           if (!__all_sync(0xffffffffu, mbar_wait(acc_full(b), (uint32_t)(u & 1), f.spin))) {
             atomicOr(f.status, 1u);
-            s_err = 1;
+                s_err = 1;
             break;
           }
           asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
           const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * 256);
           const int lrow = t * TCM + q * 32 + lane;  // row within the batch
           if (!last) {
-            // bias + GELU -> BF16 -> this row of the output scratch
-            bf16 *hrow = f.act + (long long)(h_row0 + lrow) * f.hidden;
-            uint32_t va[16], vb[16];
-            tmem_ld16(va, tbase + c_begin);
+            // bias + GELU -> BF16 staging -> TMA store into the scratch rows
+            TcArgs g{};
+            const int chunks = (N / 2) / 32;
+            auto emit = [&](const uint32_t (&v)[32], int c0) {
+              unsigned char *st = my_stage + sbuf * 2048;
+              sbuf ^= 1;
+              if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 1;\n" ::: "memory");
+              __syncwarp();
+              epilogue32<kTcBiasGelu>(g, v, 0, 0, c0, sBias, st, lane);
+              asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+              __syncwarp();
+              if (lane == 0) {
+                asm volatile(
+                    "cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%2, %3, %4}], [%1];\n" ::"l"(
+                        reinterpret_cast<uint64_t>(&tmH)),
+                    "r"(smem_u32(st)), "r"(c0), "r"(h_row0 + t * TCM + q * 32), "r"(0)
+                    : "memory");
+                asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+              }
+            };
+            uint32_t va[32], vb[32];
+            tmem_ld32(va, tbase + c_begin);
             tmem_wait();
-            for (int c = 0; c < cpp; c += 32) {
-              if (c + 16 < cpp) tmem_ld16(vb, tbase + c_begin + c + 16);
-              fused_gelu16(va, sBias, c_begin + c, hrow + c_begin + c);
+            for (int c = 0; c < chunks; c += 2) {
+              if (c + 1 < chunks) tmem_ld32(vb, tbase + c_begin + (c + 1) * 32);
+              emit(va, c_begin + c * 32);
               tmem_wait();
-              if (c + 16 < cpp) {
-                if (c + 32 < cpp) tmem_ld16(va, tbase + c_begin + c + 32);
-                fused_gelu16(vb, sBias, c_begin + c + 16, hrow + c_begin + c + 16);
+              if (c + 1 < chunks) {
+                if (c + 2 < chunks) tmem_ld32(va, tbase + c_begin + (c + 2) * 32);
+                emit(vb, c_begin + (c + 1) * 32);
                 tmem_wait();
               }
             }
           } else {
             // output layer: bias -> FP32 rows of Y (real columns, real rows)
             const int grow = r0 + lrow;
-            for (int c0 = c_begin; c0 < c_begin + cpp; c0 += 4) {
-              uint32_t v[4];
-              tmem_ld4(v, tbase + (uint32_t)c0);
+            for (int c0 = c_begin; c0 < c_begin + N / 2; c0 += 8) {
+              uint32_t v[8];
+              asm volatile(
+                  "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+                  : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+                    "=r"(v[6]), "=r"(v[7])
+                  : "r"(tbase + (uint32_t)c0));
               tmem_wait();
               if (lrow >= rows) continue;
               float *y = f.Y + ((long long)z * f.n + grow) * nv;
 #pragma unroll
-              for (int i = 0; i < 4; ++i)
+              for (int i = 0; i < 8; ++i)
                 if (c0 + i < nv) y[c0 + i] = __uint_as_float(v[i]) + sBias[c0 + i];
             }
           }
@@ -1142,11 +1115,13 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
           mbar_arrive(acc_empty(b));
         }
       }
-      // ---- pass end: copies and stores complete (and the scratch stores
-      // ordered before the async proxy's reads) before the next pass reads
-      // the scratch or reuses the ring and barriers
+      // ---- pass end: copies and stores complete before the next pass reads
+      // the scratch or reuses the ring, staging and barriers
       asm volatile("cp.async.wait_all;\n" ::: "memory");
-      asm volatile("fence.proxy.async.global;\n" ::: "memory");
+      if (warp >= 4 && lane == 0) {
+        asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
+        asm volatile("fence.proxy.async.global;\n" ::: "memory");
+      }
       asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
       __syncthreads();
       failed = s_err != 0;  // a timeout: stop after this drained pass
@@ -1585,10 +1560,9 @@ int check_status(mcml_mlp *p) {
 }
 
 // Whole-network inference (tc_fused_forward_kernel) applies when every
-// hidden layer can stream its activations by TMA in 64-column chunks and
-// its epilogue parts (a quarter of the columns each) are whole 16-column
-// loads: hidden width a multiple of 64, at most kMaxFusedLayers layers, an
-// output of at most 16 columns.
+// hidden layer can stream its activations by TMA and store them in 32-column
+// TMA tiles: hidden width a multiple of 64, at most kMaxFusedLayers layers,
+// an output of at most 16 columns.
 bool fused_eligible(const mcml_mlp *p) {
   return p->hidden % 64 == 0 && p->hidden <= 256 && p->layers <= kMaxFusedLayers &&
          p->out_dim <= 16 && p->in_pad <= 256;
@@ -1631,10 +1605,12 @@ int fused_predict(mcml_mlp *p, const float *X, uint64_t n, float *mean, float *s
     MLP_TRY(cudaMalloc(&p->d_fy, p->E * rows_cap * p->out_dim * sizeof(float)));
     p->fcap = rows_cap;
   }
-  CUtensorMap amap;
+  CUtensorMap amap, hmap;
   std::memset(&amap, 0, sizeof(amap));
-  if (!encode_act_map(p, scratch_rows, 64, TCM, CU_TENSOR_MAP_SWIZZLE_128B, &amap))
-    return set_error(MCML_E_CUDA, "mlp: tensor map of the activation scratch");
+  std::memset(&hmap, 0, sizeof(hmap));
+  if (!encode_act_map(p, scratch_rows, 64, TCM, CU_TENSOR_MAP_SWIZZLE_128B, &amap) ||
+      !encode_act_map(p, scratch_rows, 32, 32, CU_TENSOR_MAP_SWIZZLE_64B, &hmap))
+    return set_error(MCML_E_CUDA, "mlp: tensor maps of the activation scratch");
   FusedArgs f;
   std::memset(&f, 0, sizeof(f));
   f.layers = p->layers;
@@ -1653,10 +1629,9 @@ int fused_predict(mcml_mlp *p, const float *X, uint64_t n, float *mean, float *s
   f.W = p->d_w16;
   f.Wf = p->d_w;
   f.strideW = p->stride;
-  f.act = p->d_act;
   f.status = p->d_status;
   f.spin = p->spin;
-  const size_t fixed = tc_align1k((size_t)maxKN * 2) + kTcSmemFixed + 1024;
+  const size_t fixed = tc_align1k((size_t)maxKN * 2) + kTcStageBytes + kTcSmemFixed + 1024;
   const size_t slot = tc_slot_bytes(64);
   f.slots = (int)std::min<size_t>(16, (kTcSmemMax - fixed) / slot);
   if (f.slots < 2) return set_error(MCML_E_INVALID, "mlp: layers too wide for the fused forward");
@@ -1676,8 +1651,8 @@ int fused_predict(mcml_mlp *p, const float *X, uint64_t n, float *mean, float *s
     f.n = rows;
     f.X = p->d_fx;
     f.Y = p->d_fy;
-    tc_fused_forward_kernel<<<dim3(per_member, 1, p->E), kFusedThreads, smem, p->stream>>>(f,
-                                                                                         amap);
+    tc_fused_forward_kernel<<<dim3(per_member, 1, p->E), kTcWarps * 32, smem, p->stream>>>(f, amap,
+                                                                                        hmap);
     MLP_TRY(cudaGetLastError());
     ensemble_kernel<<<(unsigned)(((long long)rows * p->out_dim + 255) / 256), 256, 0, p->stream>>>(
         p->d_fy, (long long)rows * p->out_dim, p->E, (long long)rows * p->out_dim, p->d_tmean,

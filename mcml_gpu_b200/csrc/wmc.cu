@@ -71,10 +71,13 @@ __device__ __forceinline__ float ex2(float x) {
 // features sit interleaved in shared memory, {F_jk, F_j+1,k}, so that one
 // 16-byte load feeds two k and every contraction step is one paired FMA
 // (__ffma2_rn) over the two photons against the combo's coefficient held
-// twice in a register pair.  Two pairs are taken per iteration, which
-// gives each thread 2*kPer independent FMA chains.  Per term that is K/2
-// paired FMAs, one MUFU exp2, half a paired add and K/(4*kPer) shared
-// loads; the FP32 lanes (K+1 operations per term) are the binding unit.
+// twice in a register pair.  A photon's exponent starts at its log2 weight
+// (feature K-2, coefficient 1) and takes the 2L = K-2 pathlength and
+// interaction terms, so the unit coefficient and the zero padding column
+// cost nothing.  Two pairs are taken per iteration, which gives each
+// thread 2*kPer independent FMA chains.  Per term that is L paired FMAs,
+// one MUFU exp2, half a paired add and 1.5 shared loads; the FP32 lanes
+// (2L + 1 operations per term) are the binding unit.
 template <int K>
 __global__ void __launch_bounds__(kThreads, 4) wmc_kernel(const float *F, uint64_t D,
                                                        const float *coef, uint64_t C,
@@ -148,9 +151,10 @@ __global__ void __launch_bounds__(kThreads, 4) wmc_kernel(const float *F, uint64
 #pragma unroll
       for (int h = 0; h < 2; ++h)
 #pragma unroll
-        for (int r = 0; r < kPer; ++r) e[h][r] = make_float2(0.0f, 0.0f);
+        for (int r = 0; r < kPer; ++r)
+          e[h][r] = *reinterpret_cast<const float2 *>(&sF[cur][jp + h][K - 2]);  // log2 w
 #pragma unroll
-      for (int k = 0; k < K; k += 2) {
+      for (int k = 0; k < K - 2; k += 2) {
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
           const float4 f = *reinterpret_cast<const float4 *>(&sF[cur][jp + h][k]);
