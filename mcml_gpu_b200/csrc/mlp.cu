@@ -782,64 +782,111 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1)
 // Whole-network forward for inference on the tensor cores: every layer of
 // every member in one launch.  CTA (c, member z) takes batches of
 // batch_rows rows (whole 128-row tiles) and runs each batch through all the
-// layers before the next batch.  Per layer it loads that layer's weights
-// (the B operand, MN-major, no swizzle) and bias into shared memory, streams
-// the batch's activations in (layer 0: the normalised inputs by cp.async;
-// later layers: the CTA's own scratch rows by TMA, 128-byte swizzle) and
-// writes the layer's output back to its scratch (hidden layers: bias +
-// GELU, BF16, TMA stores) or to Y (the output layer: bias, FP32).  A CTA's
-// scratch (2 x batch_rows rows, ping-pong between layers) is read back by
-// the same CTA right after it was written, so the activations stay in L2
-// between layers instead of making an HBM round trip per layer, and one
-// launch replaces one per layer per chunk.  Roles, barriers and the
-// bounded waits are those of tc_layer_kernel; the barriers are set up
-// afresh for every (batch, layer) pass, after the previous pass drained.
+// layers before the next batch.  A (batch, layer) pair is a *pass*.  The
+// batch's activations ping-pong through the CTA's own scratch rows (two
+// buffers of batch_rows rows, L2-resident) between layers; every A operand
+// (layer 0: the normalised inputs, padded to 64 columns; later layers: the
+// scratch) streams in by TMA in 64-column chunks, 128-byte swizzled.
+//
+// Roles (12 warps), all running through the same sequence of passes with
+// no block-wide barrier between passes:
+//  * warp 0, lane 0 -- A producer: chunk loads into a ring of shared-memory
+//    slots (a_full / a_empty).  Before loading tile t of layer l > 0 it
+//    waits h_done[t], which the epilogue completes once layer l-1's stores
+//    of tile t have finished.
+//  * warp 3, lane 0 -- MMA issuer: per pass it waits for the layer's
+//    weights (w_full), issues the tiles' tcgen05.mma into two 256-column
+//    tensor-memory accumulators (acc_full / acc_empty), and once the pass's
+//    MMAs have completed (mma_done) brings the next pass's weights in with
+//    bulk copies of their packed image -- while the epilogue still works on
+//    the pass's last tile.
+//  * warps 4-11 -- epilogue: bias + GELU into 64-byte-swizzled staging
+//    tiles written out by TMA stores (hidden layers), or bias into FP32
+//    rows of Y (the output layer).  The epilogue threads copy each pass's
+//    bias into one of three shared-memory buffers (bias_ready): the
+//    double-buffered accumulators keep the slowest epilogue thread within
+//    two tiles, so within two passes, of the fastest.
+// The mbarriers are set up once; every phase is derived from counters that
+// run across passes.  Every wait is bounded: a timeout sets *status and
+// s_err, and every role stops at its next check; the CTA then drains its
+// copies and MMAs before it frees tensor memory.
 constexpr int kMaxFusedLayers = 12;
+constexpr int kFusedMaxTiles = 16;  // batch_rows / 128
 
 struct FusedArgs {
   int n;                // rows
   int layers;           // weight matrices (depth + 1)
-  int ctas_per_member;  // gridDim.x
-  int batch_rows;       // rows per batch, a multiple of 128
-  int hidden;           // scratch row width (BF16 elements)
-  int K[kMaxFusedLayers], N[kMaxFusedLayers], n_valid[kMaxFusedLayers];
-  long long w_off[kMaxFusedLayers], b_off[kMaxFusedLayers];
-  const bf16 *X;        // n x K[0], normalised inputs shared by the members
-  const bf16 *W;        // BF16 parameters of member 0; member z at z * strideW
-  const float *Wf;      // FP32 parameters (the biases)
+  int batch_rows;       // rows per batch, a multiple of 128, at most 128 * kFusedMaxTiles
+  int K[kMaxFusedLayers];         // contraction widths, multiples of 64
+  int N[kMaxFusedLayers];         // MMA widths, multiples of 16, at most 256
+  int n_valid[kMaxFusedLayers];   // real output columns
+  long long img_off[kMaxFusedLayers];  // byte offset of a layer's B image in a member's image
+  long long b_off[kMaxFusedLayers];    // bias offsets in a member's FP32 parameters
+  const unsigned char *img;       // packed B images, member z at z * img_stride
+  long long img_stride;
+  const float *Wf;                // FP32 parameters (the biases); member z at z * strideW
   long long strideW;
-  float *Y;             // members x n x n_valid[last]
-  int slots;            // A ring slots
+  float *Y;                       // members x n x n_valid[last]
+  int slots;                      // A ring slots
   unsigned *status;
   long long spin;
 };
 
+// Global -> shared bulk copy (no tensor map) completing on an mbarrier.
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes,
+                                         uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+          dst),
+      "l"(src), "r"(bytes), "r"(bar)
+      : "memory");
+}
+
 __global__ void __launch_bounds__(kTcWarps * 32, 1)
-    tc_fused_forward_kernel(const FusedArgs f, const __grid_constant__ CUtensorMap tmA,
+    tc_fused_forward_kernel(const FusedArgs f, const __grid_constant__ CUtensorMap tmX,
+                            const __grid_constant__ CUtensorMap tmA,
                             const __grid_constant__ CUtensorMap tmH) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char *smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int z = blockIdx.z;
   const int nslots = f.slots;
-  const uint32_t slot_stride = 64 / 8 * kLboA;  // room for the widest chunk
-  // shared memory sized for the widest layer: B operand, A ring, staging,
-  // bias, barriers, TMEM slot
-  int maxKN = 0;
-  for (int l = 0; l < f.layers; ++l) maxKN = max(maxKN, f.K[l] * f.N[l]);
+  constexpr uint32_t kSlot = 64 / 8 * kLboA;  // one 64-column x 128-row chunk
+  int maxB = 0;
+  for (int l = 0; l < f.layers; ++l) maxB = max(maxB, f.K[l] * f.N[l] * 2);
   unsigned char *sB = smem;
-  unsigned char *sA = smem + (((size_t)maxKN * 2 + 1023) & ~(size_t)1023);
-  unsigned char *sStage = sA + (size_t)nslots * slot_stride;
-  float *sBias = reinterpret_cast<float *>(sStage + (size_t)8 * 2 * 2048);
-  uint64_t *bars = reinterpret_cast<uint64_t *>(sBias + 256);
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 37);
+  unsigned char *sA = smem + (((size_t)maxB + 1023) & ~(size_t)1023);
+  unsigned char *sStage = sA + (size_t)nslots * kSlot;
+  float *sBias = reinterpret_cast<float *>(sStage + (size_t)8 * 2048);  // [3][256]
+  uint64_t *bars = reinterpret_cast<uint64_t *>(sBias + 3 * 256);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 58);
   const uint32_t sA_u = smem_u32(sA), sB_u = smem_u32(sB), bars_u = smem_u32(bars);
   auto a_full = [&](int s) { return bars_u + 8u * s; };
   auto a_empty = [&](int s) { return bars_u + 8u * (16 + s); };
   auto acc_full = [&](int b) { return bars_u + 8u * (32 + b); };
   auto acc_empty = [&](int b) { return bars_u + 8u * (34 + b); };
-  const uint32_t drain_bar = bars_u + 8u * 36;
+  const uint32_t w_full = bars_u + 8u * 36;
+  const uint32_t mma_done = bars_u + 8u * 37;
+  auto h_done = [&](int t) { return bars_u + 8u * (38 + t); };
+  auto bias_ready = [&](int i) { return bars_u + 8u * (54 + i); };  // 3 of the 4 used
+  volatile int &s_err = *reinterpret_cast<volatile int *>(tslot + 1);
 
+  if (tid == 0) {
+    s_err = 0;
+    for (int c = 0; c < nslots; ++c) {
+      mbar_init(a_full(c), 1);
+      mbar_init(a_empty(c), 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(acc_full(b), 1);
+      mbar_init(acc_empty(b), 256);
+    }
+    mbar_init(w_full, 1);
+    mbar_init(mma_done, 1);
+    for (int t = 0; t < kFusedMaxTiles; ++t) mbar_init(h_done(t), 8);
+    for (int i = 0; i < 3; ++i) mbar_init(bias_ready(i), 256);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
   if (warp == 0) {  // two 256-column accumulators: all of tensor memory
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
                      smem_u32(tslot)),
@@ -847,292 +894,326 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
   }
-  const int cta = z * gridDim.x + blockIdx.x;
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t tmem = *tslot;
+
+  const int L = f.layers;
   const int BR = f.batch_rows;
   const int batches = (f.n + BR - 1) / BR;
-  const bf16 *Wz = f.W + (long long)z * f.strideW;
-  const float *Wfz = f.Wf + (long long)z * f.strideW;
-  // a wait of this CTA timed out (written by the role, read after a barrier);
-  // beside the TMEM slot in the fixed part of the dynamic shared memory
-  volatile int &s_err = *reinterpret_cast<volatile int *>(tslot + 1);
-  if (tid == 0) s_err = 0;
-  bool inited = false;
-  bool failed = false;
-
-  for (int bt = blockIdx.x; bt < batches && !failed; bt += gridDim.x) {
-    const int r0 = bt * BR;                       // first row of the batch
+  const int nb = (int)blockIdx.x < batches
+                     ? (batches - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x
+                     : 0;
+  const int passes = nb * L;
+  const int cta = z * gridDim.x + blockIdx.x;
+  // the rows and tiles of pass wp's batch
+  auto pass_rows = [&](int wp, int &r0, int &tiles) {
+    const int bt = (int)blockIdx.x + (wp / L) * (int)gridDim.x;
+    r0 = bt * BR;
     const int rows = min(BR, f.n - r0);
-    const int tiles = (rows + TCM - 1) / TCM;
-    for (int l = 0; l < f.layers && !failed; ++l) {
-      const int K = f.K[l], N = f.N[l], nv = f.n_valid[l];
-      const bool last = l == f.layers - 1;
-      const int KC = tc_chunk_k(K);
-      const int nch = K / KC;
-      const uint32_t lboB = (uint32_t)(N / 8) * 128;
-      const bool tma = l > 0 && K % 64 == 0;
-      // scratch rows: input buffer (l-1)%2, output buffer l%2
-      const int a_row0 = (cta * 2 + ((l + 1) & 1)) * BR;
-      const int h_row0 = (cta * 2 + (l & 1)) * BR;
-      // ---- pass set-up: barriers afresh, this layer's weights and bias
-      __syncthreads();
-      if (tid == 0) {
-        // the previous pass completed every phase it started (no timeout,
-        // or the kernel would have stopped), so nothing arrives on these
-        if (inited) {
-          for (int c = 0; c < nslots; ++c) {
-            asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(a_full(c)) : "memory");
-            asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(a_empty(c)) : "memory");
-          }
-          for (int b = 0; b < 2; ++b) {
-            asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(acc_full(b)) : "memory");
-            asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(acc_empty(b)) : "memory");
-          }
-          asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(drain_bar) : "memory");
-        }
-        for (int c = 0; c < nslots; ++c) {
-          mbar_init(a_full(c), tma ? 1 : kProducers);
-          mbar_init(a_empty(c), 1);
-        }
-        for (int b = 0; b < 2; ++b) {
-          mbar_init(acc_full(b), 1);
-          mbar_init(acc_empty(b), 256);
-        }
-        mbar_init(drain_bar, 1);
-        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-      }
-      inited = true;
-      const bf16 *W = Wz + f.w_off[l];
-      if (nv == N) {
-        const int nc8 = N / 8;
-        for (int c = tid; c < K * nc8; c += kTcWarps * 32) {
-          const int k_lo = c & 7, rest = c >> 3;
-          const int nc = rest % nc8, k = (rest / nc8) * 8 + k_lo;
-          const uint32_t dst = sB_u + (k >> 3) * lboB + nc * 128 + k_lo * 16;
-          const bf16 *src = W + (long long)k * N + nc * 8;
-          asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src)
-                       : "memory");
-        }
-      } else {
-        bf16 *sb = reinterpret_cast<bf16 *>(sB);
-        for (int e = tid; e < K * N; e += kTcWarps * 32) {
-          const int k = e / N, nn = e % N;
-          const bf16 v = nn < nv ? W[(long long)k * nv + nn] : __float2bfloat16(0.0f);
-          sb[((k >> 3) * lboB + (nn >> 3) * 128 + (k & 7) * 16 + (nn & 7) * 2) / 2] = v;
-        }
-      }
-      for (int c = tid; c < N; c += kTcWarps * 32) sBias[c] = c < nv ? Wfz[f.b_off[l] + c] : 0.0f;
-      asm volatile("cp.async.wait_all;\n" ::: "memory");
-      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-      asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-      __syncthreads();
-      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-      const uint32_t tmem = *tslot;
+    tiles = (rows + TCM - 1) / TCM;
+  };
 
-      if (warp < 3 && tma) {
-        // ---- producer: this CTA's scratch rows of the layer's input
-        if (tid == 0) {
-          int gi = 0;
-          bool alive = true;
-          for (int t = 0; t < tiles && alive; ++t) {
-            for (int c = 0; c < nch; ++c, ++gi) {
-              const int slot = gi % nslots, use = gi / nslots;
-              if (use > 0 && !mbar_wait(a_empty(slot), (uint32_t)((use - 1) & 1), f.spin)) {
-                atomicOr(f.status, 1u);
-                s_err = 1;
-                alive = false;
-                break;
-              }
-              const uint32_t dst = sA_u + (uint32_t)slot * slot_stride;
-              const uint32_t bytes = (uint32_t)(KC / 8) * kLboA;
-              asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(
-                               a_full(slot)),
-                           "r"(bytes)
-                           : "memory");
-              asm volatile(
-                  "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-                  " [%0], [%1, {%3, %4, %5}], [%2];\n" ::"r"(dst),
-                  "l"(reinterpret_cast<uint64_t>(&tmA)), "r"(a_full(slot)), "r"(c * KC),
-                  "r"(a_row0 + t * TCM), "r"(0)
-                  : "memory");
-            }
-          }
-          for (int slot = 0; slot < nslots && slot < gi; ++slot) {
-            const int last_use = (gi - 1 - slot) / nslots;
-            if (!mbar_wait(a_full(slot), (uint32_t)(last_use & 1), kTcDrainSpin))
-              { atomicOr(f.status, 2u); s_err = 1; }
-          }
-        }
-        __syncwarp();
-      } else if (warp < 3) {
-        // ---- producers (layer 0): the normalised inputs by cp.async,
-        // rows past n as zeros
-        const int per_chunk = TCM * KC / 8;
-        int gi = 0;
-        for (int t = 0; t < tiles; ++t) {
-          const int m0 = r0 + t * TCM;
-          bool alive = true;
-          for (int c = 0; c < nch; ++c, ++gi) {
-            const int slot = gi % nslots, use = gi / nslots;
-            if (use > 0 && !mbar_wait(a_empty(slot), (uint32_t)((use - 1) & 1), f.spin)) {
+  if (warp == 0) {
+    // ---- A producer
+    if (lane == 0) {
+      int gi = 0;  // chunk sequence number over all passes
+      bool alive = true;
+      for (int wp = 0; wp < passes && alive; ++wp) {
+        const int j = wp / L, l = wp % L;
+        int r0, tiles;
+        pass_rows(wp, r0, tiles);
+        const int nch = f.K[l] / 64;
+        const int a_row0 = (cta * 2 + ((l + 1) & 1)) * BR;  // layer l-1's output buffer
+        for (int t = 0; t < tiles && alive; ++t) {
+          if (l > 0) {
+            // layer l-1's stores of this tile are complete (completion
+            // number j*(L-1) + l-1 of h_done[t]: one per hidden layer and batch)
+            if (s_err || !mbar_wait(h_done(t), (uint32_t)((j * (L - 1) + l - 1) & 1), f.spin)) {
               atomicOr(f.status, 1u);
-                s_err = 1;
+              s_err = 1;
               alive = false;
               break;
             }
-            const uint32_t base = sA_u + (uint32_t)slot * slot_stride;
-            for (int e = tid; e < per_chunk; e += kProducers) {
-              const int r_lo = e & 7, rest = e >> 3;
-              const int kl = rest % (KC / 8), r = (rest / (KC / 8)) * 8 + r_lo;
-              const uint32_t dst = base + kl * kLboA + (r >> 3) * 128 + r_lo * 16;
-              const int gr = m0 + r;
-              const bf16 *src = f.X + (long long)(gr < f.n ? gr : 0) * K + (c * (KC / 8) + kl) * 8;
-              const uint32_t bytes = gr < f.n ? 16u : 0u;
-              asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src),
-                           "r"(bytes)
-                           : "memory");
-            }
-            asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(
-                             a_full(slot))
-                         : "memory");
+            asm volatile("fence.proxy.async.global;\n" ::: "memory");
           }
-          if (!alive) break;
-        }
-      } else if (warp == 3) {
-        // ---- MMA issuer
-        if (lane == 0) {
-          const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 16) |
-                                 ((uint32_t)(N >> 3) << 17) | ((uint32_t)(TCM >> 4) << 24);
-          for (int t = 0; t < tiles; ++t) {
-            const int b = t & 1, u = t >> 1;
-            if (u > 0 && !mbar_wait(acc_empty(b), (uint32_t)((u - 1) & 1), f.spin)) {
+          for (int c = 0; c < nch; ++c, ++gi) {
+            const int slot = gi % nslots, use = gi / nslots;
+            if (use > 0 &&
+                (s_err || !mbar_wait(a_empty(slot), (uint32_t)((use - 1) & 1), f.spin))) {
               atomicOr(f.status, 1u);
-                s_err = 1;
+              s_err = 1;
+              alive = false;
               break;
             }
-            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-            const uint32_t d = tmem + (uint32_t)(b * 256);
-            bool ok = true;
-            for (int c = 0; c < nch && ok; ++c) {
-              const int gi = t * nch + c, slot = gi % nslots, use = gi / nslots;
-              if (!mbar_wait(a_full(slot), (uint32_t)(use & 1), f.spin)) {
-                atomicOr(f.status, 1u);
-                s_err = 1;
-                ok = false;
-                break;
-              }
-              asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-              const uint32_t base = sA_u + (uint32_t)slot * slot_stride;
-              for (int j = 0; j < KC / 16; ++j) {
-                const int ks = c * (KC / 16) + j;
-                const uint64_t ad = tma ? umma_desc_sw128(base + 32 * j)
-                                        : umma_desc(base + 2 * j * kLboA, kLboA, 128);
-                const uint64_t bd = umma_desc(sB_u + 2 * ks * lboB, lboB, 128);
-                const uint32_t acc = ks > 0 ? 1u : 0u;
-                asm volatile(
-                    "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-                    " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d),
-                    "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
-                    : "memory");
-              }
-              umma_commit(a_empty(slot));
-            }
-            if (!ok) break;
-            umma_commit(acc_full(b));
+            const uint32_t dst = sA_u + (uint32_t)slot * kSlot;
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(
+                             a_full(slot)),
+                         "r"(kSlot)
+                         : "memory");
+            const uint64_t map = l == 0 ? reinterpret_cast<uint64_t>(&tmX)
+                                        : reinterpret_cast<uint64_t>(&tmA);
+            const int row = l == 0 ? r0 + t * TCM : a_row0 + t * TCM;
+            asm volatile(
+                "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+                " [%0], [%1, {%3, %4, %5}], [%2];\n" ::"r"(dst),
+                "l"(map), "r"(a_full(slot)), "r"(c * 64), "r"(row), "r"(0)
+                : "memory");
           }
-          umma_commit(drain_bar);
-          if (!mbar_wait(drain_bar, 0u, kTcDrainSpin)) { atomicOr(f.status, 2u); s_err = 1; }
         }
-        __syncwarp();
-      } else {
-        // ---- epilogue: warp w drains TMEM lanes 32*(w%4).., column half (w-4)/4
-        const int q = warp & 3, half = (warp - 4) >> 2;
-        const int c_begin = half * (N / 2);
-        unsigned char *my_stage = sStage + (warp - 4) * 4096;
-        int sbuf = 0;  // staging tile of the next store, alternating as in tc_layer_kernel
-        for (int t = 0; t < tiles; ++t) {
-          const int b = t & 1, u = t >> 1;
-          if (!__all_sync(0xffffffffu, mbar_wait(acc_full(b), (uint32_t)(u & 1), f.spin))) {
+      }
+      // drain: every load issued has landed (its slot's a_full phase)
+      for (int slot = 0; slot < nslots && slot < gi; ++slot) {
+        const int last_use = (gi - 1 - slot) / nslots;
+        if (!mbar_wait(a_full(slot), (uint32_t)(last_use & 1), kTcDrainSpin)) {
+          atomicOr(f.status, 2u);
+          s_err = 1;
+        }
+      }
+    }
+    __syncwarp();
+  } else if (warp == 3) {
+    // ---- MMA issuer (and the weight loads)
+    if (lane == 0) {
+      const unsigned char *img = f.img + (long long)z * f.img_stride;
+      auto load_weights = [&](int wp) {
+        const int l = wp % L;
+        const uint32_t bytes = (uint32_t)(f.K[l] * f.N[l] * 2);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(w_full),
+                     "r"(bytes)
+                     : "memory");
+        for (uint32_t off = 0; off < bytes; off += 32768u)
+          bulk_g2s(sB_u + off, img + f.img_off[l] + off, min(32768u, bytes - off), w_full);
+      };
+      int gi = 0, tseq = 0;
+      int w_pending = -1;  // pass whose weights were requested and not yet waited for
+      if (passes > 0) {
+        load_weights(0);
+        w_pending = 0;
+      }
+      bool alive = true;
+      for (int wp = 0; wp < passes && alive; ++wp) {
+        const int l = wp % L;
+        int r0, tiles;
+        pass_rows(wp, r0, tiles);
+        (void)r0;
+        if (s_err || !mbar_wait(w_full, (uint32_t)(wp & 1), f.spin)) {
+          atomicOr(f.status, 1u);
+          s_err = 1;
+          break;
+        }
+        w_pending = -1;
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        const int N = f.N[l], nch = f.K[l] / 64;
+        const uint32_t lboB = (uint32_t)(N / 8) * 128;
+        const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 16) |
+                               ((uint32_t)(N >> 3) << 17) | ((uint32_t)(TCM >> 4) << 24);
+        for (int t = 0; t < tiles && alive; ++t, ++tseq) {
+          const int b = tseq & 1, u = tseq >> 1;
+          if (u > 0 && (s_err || !mbar_wait(acc_empty(b), (uint32_t)((u - 1) & 1), f.spin))) {
             atomicOr(f.status, 1u);
-                s_err = 1;
+            s_err = 1;
+            alive = false;
             break;
           }
           asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-          const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * 256);
-          const int lrow = t * TCM + q * 32 + lane;  // row within the batch
-          if (!last) {
-            // bias + GELU -> BF16 staging -> TMA store into the scratch rows
-            TcArgs g{};
-            const int chunks = (N / 2) / 32;
-            auto emit = [&](const uint32_t (&v)[32], int c0) {
-              unsigned char *st = my_stage + sbuf * 2048;
-              sbuf ^= 1;
-              if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 1;\n" ::: "memory");
-              __syncwarp();
-              epilogue32<kTcBiasGelu>(g, v, 0, 0, c0, sBias, st, lane);
-              asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-              __syncwarp();
-              if (lane == 0) {
-                asm volatile(
-                    "cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%2, %3, %4}], [%1];\n" ::"l"(
-                        reinterpret_cast<uint64_t>(&tmH)),
-                    "r"(smem_u32(st)), "r"(c0), "r"(h_row0 + t * TCM + q * 32), "r"(0)
-                    : "memory");
-                asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
-              }
-            };
-            uint32_t va[32], vb[32];
-            tmem_ld32(va, tbase + c_begin);
-            tmem_wait();
-            for (int c = 0; c < chunks; c += 2) {
-              if (c + 1 < chunks) tmem_ld32(vb, tbase + c_begin + (c + 1) * 32);
-              emit(va, c_begin + c * 32);
-              tmem_wait();
-              if (c + 1 < chunks) {
-                if (c + 2 < chunks) tmem_ld32(va, tbase + c_begin + (c + 2) * 32);
-                emit(vb, c_begin + (c + 1) * 32);
-                tmem_wait();
-              }
+          const uint32_t d = tmem + (uint32_t)(b * 256);
+          for (int c = 0; c < nch; ++c, ++gi) {
+            const int slot = gi % nslots, use = gi / nslots;
+            if (s_err || !mbar_wait(a_full(slot), (uint32_t)(use & 1), f.spin)) {
+              atomicOr(f.status, 1u);
+              s_err = 1;
+              alive = false;
+              break;
             }
-          } else {
-            // output layer: bias -> FP32 rows of Y (real columns, real rows)
-            const int grow = r0 + lrow;
-            for (int c0 = c_begin; c0 < c_begin + N / 2; c0 += 8) {
-              uint32_t v[8];
-              asm volatile(
-                  "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
-                  : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
-                    "=r"(v[6]), "=r"(v[7])
-                  : "r"(tbase + (uint32_t)c0));
-              tmem_wait();
-              if (lrow >= rows) continue;
-              float *y = f.Y + ((long long)z * f.n + grow) * nv;
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            const uint32_t base = sA_u + (uint32_t)slot * kSlot;
 #pragma unroll
-              for (int i = 0; i < 8; ++i)
-                if (c0 + i < nv) y[c0 + i] = __uint_as_float(v[i]) + sBias[c0 + i];
+            for (int jj = 0; jj < 4; ++jj) {
+              const int ks = c * 4 + jj;
+              const uint64_t ad = umma_desc_sw128(base + 32 * jj);
+              const uint64_t bd = umma_desc(sB_u + 2 * ks * lboB, lboB, 128);
+              const uint32_t acc = ks > 0 ? 1u : 0u;
+              asm volatile(
+                  "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                  " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d),
+                  "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+                  : "memory");
             }
+            umma_commit(a_empty(slot));
           }
-          asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-          mbar_arrive(acc_empty(b));
+          if (alive) umma_commit(acc_full(b));
+        }
+        // every MMA of this pass (issued so far) has read the weights
+        umma_commit(mma_done);
+        if (!mbar_wait(mma_done, (uint32_t)(wp & 1), kTcDrainSpin)) {
+          atomicOr(f.status, 2u);
+          s_err = 1;
+          alive = false;
+        }
+        if (alive && wp + 1 < passes) {
+          load_weights(wp + 1);
+          w_pending = wp + 1;
         }
       }
-      // ---- pass end: copies and stores complete before the next pass reads
-      // the scratch or reuses the ring, staging and barriers
-      asm volatile("cp.async.wait_all;\n" ::: "memory");
-      if (warp >= 4 && lane == 0) {
+      if (w_pending >= 0 && !mbar_wait(w_full, (uint32_t)(w_pending & 1), kTcDrainSpin)) {
+        atomicOr(f.status, 2u);
+        s_err = 1;
+      }
+    }
+    __syncwarp();
+  } else if (warp >= 4) {
+    // ---- epilogue: warp w drains TMEM lanes 32*(w%4).., column half (w-4)/4
+    const int q = warp & 3, half = (warp - 4) >> 2;
+    unsigned char *my_stage = sStage + (warp - 4) * 2048;  // one staging tile per warp
+    int pend = -1;    // lane 0: tile whose stores are issued but not yet signalled
+    auto signal_stored = [&]() {
+      if (lane == 0 && pend >= 0) {
         asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
         asm volatile("fence.proxy.async.global;\n" ::: "memory");
+        mbar_arrive(h_done(pend));
+        pend = -1;
       }
-      asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-      __syncthreads();
-      failed = s_err != 0;  // a timeout: stop after this drained pass
+    };
+    int tseq = 0;
+    bool alive = true;
+    for (int wp = 0; wp < passes && alive; ++wp) {
+      const int l = wp % L;
+      const bool last = l == L - 1;
+      int r0, tiles;
+      pass_rows(wp, r0, tiles);
+      const int N = f.N[l], nv = f.n_valid[l];
+      const int rows = min(BR, f.n - r0);
+      const int c_begin = half * (N / 2);
+      const int h_row0 = (cta * 2 + (l & 1)) * BR;
+      // this pass's bias into buffer wp % 3, completed on bias_ready
+      float *bias = sBias + (wp % 3) * 256;
+      {
+        const int e = tid - 128;  // 0..255
+        bias[e] = e < nv ? f.Wf[(long long)z * f.strideW + f.b_off[l] + e] : 0.0f;
+        mbar_arrive(bias_ready(wp % 3));
+        if (s_err || !mbar_wait(bias_ready(wp % 3), (uint32_t)((wp / 3) & 1), f.spin)) {
+          atomicOr(f.status, 1u);
+          s_err = 1;
+          alive = false;
+          break;
+        }
+      }
+      for (int t = 0; t < tiles; ++t, ++tseq) {
+        const int b = tseq & 1, u = tseq >> 1;
+        signal_stored();
+        if (!__all_sync(0xffffffffu, s_err == 0 &&
+                                         mbar_wait(acc_full(b), (uint32_t)(u & 1), f.spin))) {
+          atomicOr(f.status, 1u);
+          s_err = 1;
+          alive = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * 256);
+        const int lrow = t * TCM + q * 32 + lane;  // row within the batch
+        if (!last) {
+          // bias + GELU -> BF16 staging -> TMA store into the scratch rows
+          TcArgs g{};
+          const int chunks = (N / 2) / 32;
+          auto emit = [&](const uint32_t (&v)[32], int c0) {
+            unsigned char *st = my_stage;
+            // the previous store has finished reading the staging tile
+            if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");
+            __syncwarp();
+            epilogue32<kTcBiasGelu>(g, v, 0, 0, c0, bias, st, lane);
+            asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+            __syncwarp();
+            if (lane == 0) {
+              asm volatile(
+                  "cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%2, %3, %4}], [%1];\n" ::"l"(
+                      reinterpret_cast<uint64_t>(&tmH)),
+                  "r"(smem_u32(st)), "r"(c0), "r"(h_row0 + t * TCM + q * 32), "r"(0)
+                  : "memory");
+              asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+            }
+          };
+          uint32_t va[32], vb[32];
+          tmem_ld32(va, tbase + c_begin);
+          tmem_wait();
+          for (int c = 0; c < chunks; c += 2) {
+            if (c + 1 < chunks) tmem_ld32(vb, tbase + c_begin + (c + 1) * 32);
+            emit(va, c_begin + c * 32);
+            tmem_wait();
+            if (c + 1 < chunks) {
+              if (c + 2 < chunks) tmem_ld32(va, tbase + c_begin + (c + 2) * 32);
+              emit(vb, c_begin + (c + 1) * 32);
+              tmem_wait();
+            }
+          }
+          pend = t;
+        } else {
+          // output layer: bias -> FP32 rows of Y (real columns, real rows)
+          const int grow = r0 + lrow;
+          for (int c0 = c_begin; c0 < c_begin + N / 2; c0 += 8) {
+            uint32_t v[8];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+                  "=r"(v[6]), "=r"(v[7])
+                : "r"(tbase + (uint32_t)c0));
+            tmem_wait();
+            if (lrow >= rows) continue;
+            float *y = f.Y + ((long long)z * f.n + grow) * nv;
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+              if (c0 + i < nv) y[c0 + i] = __uint_as_float(v[i]) + bias[c0 + i];
+          }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+        mbar_arrive(acc_empty(b));
+      }
+      signal_stored();  // the pass's last tile
     }
+    if (lane == 0) asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
+    __syncwarp();
   }
+  // ---- teardown: every role has drained what it issued
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   __syncthreads();
   if (warp == 0) {
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(*tslot), "r"(512)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(512)
                  : "memory");
   }
+}
+
+// Packed B images of the fused forward: member z, layer l at
+// z * img_stride + img_off[l], element (k, n) of the K x N operand (zero
+// past the layer's fan_in rows and fan_out columns) at byte
+// (k/8)*(N/8)*128 + (n/8)*128 + (k%8)*16 + (n%8)*2 -- the MN-major
+// no-swizzle core-matrix layout the MMA reads, so one bulk copy puts it in
+// shared memory.
+struct FusedPack {
+  int layers;
+  int K[kMaxFusedLayers], N[kMaxFusedLayers], fan_in[kMaxFusedLayers], n_valid[kMaxFusedLayers];
+  long long elem_begin[kMaxFusedLayers + 1];  // element prefix over the layers (per member)
+  long long img_off[kMaxFusedLayers];
+  long long w_off[kMaxFusedLayers];
+};
+
+__global__ void fused_pack_kernel(const bf16 *W16, long long strideW, const FusedPack pk,
+                                  unsigned char *img, long long img_stride) {
+  const int z = blockIdx.z;
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= pk.elem_begin[pk.layers]) return;
+  int l = 0;
+  while (e >= pk.elem_begin[l + 1]) ++l;
+  const long long i = e - pk.elem_begin[l];
+  const int N = pk.N[l];
+  const int k = (int)(i / N), n = (int)(i % N);
+  const bf16 v = (k < pk.fan_in[l] && n < pk.n_valid[l])
+                     ? W16[(long long)z * strideW + pk.w_off[l] + (long long)k * pk.n_valid[l] + n]
+                     : __float2bfloat16(0.0f);
+  const long long byte = pk.img_off[l] + (long long)(k >> 3) * (N / 8) * 128 + (n >> 3) * 128 +
+                         (k & 7) * 16 + (n & 7) * 2;
+  *reinterpret_cast<bf16 *>(img + (long long)z * img_stride + byte) = v;
 }
 
 constexpr size_t kTcSmemMax = 227 * 1024;  // opt-in shared memory per block
@@ -1418,9 +1499,10 @@ struct mcml_mlp {
   int cap = 0;
   // whole-network inference (tc_fused_forward_kernel): inputs and outputs of
   // up to fcap rows, and the CTAs' activation scratch
-  bf16 *d_fx = nullptr;            // fcap x in_pad
+  bf16 *d_fx = nullptr;            // fcap x in_pad rounded up to 64
   float *d_fy = nullptr;           // E x fcap x out
   bf16 *d_act = nullptr;           // 2 x batch rows x hidden per CTA
+  unsigned char *d_wimg = nullptr; // packed B images of the weights (E x image)
   long long fcap = 0;
   bf16 *d_x = nullptr;             // E x cap x in_pad
   float *d_z = nullptr;            // E x depth x cap x hidden (pre-activations)
@@ -1457,6 +1539,7 @@ struct mcml_mlp {
     dfree(d_fx);
     dfree(d_fy);
     dfree(d_act);
+    dfree(d_wimg);
     if (step_exec) cudaGraphExecDestroy(step_exec);
     dfree(d_status);
     if (own_stream && stream) cudaStreamDestroy(stream);
@@ -1562,26 +1645,30 @@ int check_status(mcml_mlp *p) {
 // Whole-network inference (tc_fused_forward_kernel) applies when every
 // hidden layer can stream its activations by TMA and store them in 32-column
 // TMA tiles: hidden width a multiple of 64, at most kMaxFusedLayers layers,
-// an output of at most 16 columns.
+// an output of at most 16 columns, hidden biases at 8-byte-aligned offsets.
 bool fused_eligible(const mcml_mlp *p) {
-  return p->hidden % 64 == 0 && p->hidden <= 256 && p->layers <= kMaxFusedLayers &&
-         p->out_dim <= 16 && p->in_pad <= 256;
+  if (!(p->hidden % 64 == 0 && p->hidden <= 256 && p->layers <= kMaxFusedLayers &&
+        p->out_dim <= 16 && p->in_pad <= 256))
+    return false;
+  for (int l = 0; l + 1 < p->layers; ++l)
+    if (p->b_off[l] % 2) return false;
+  return true;
 }
 
 constexpr int kFusedBatchRows = 1024;         // rows a CTA takes through all layers at once
 constexpr long long kFusedRows = 1ll << 22;   // rows per launch
 
-// Tensor map over the activation scratch (hidden x rows BF16, one member
-// plane) with the given box and swizzle.
-bool encode_act_map(const mcml_mlp *p, long long rows, cuuint32_t bx, cuuint32_t by,
-                    CUtensorMapSwizzle sw, CUtensorMap *map) {
+// Tensor map over a BF16 row-major array (cols x rows, one plane) with the
+// given box and swizzle.
+bool encode_rows_map(void *base, long long cols, long long rows, cuuint32_t bx, cuuint32_t by,
+                     CUtensorMapSwizzle sw, CUtensorMap *map) {
   EncodeTiledFn fn = encode_tiled();
   if (!fn) return false;
-  const cuuint64_t dims[3] = {(cuuint64_t)p->hidden, (cuuint64_t)rows, 1};
-  const cuuint64_t strides[2] = {(cuuint64_t)p->hidden * 2, (cuuint64_t)rows * p->hidden * 2};
+  const cuuint64_t dims[3] = {(cuuint64_t)cols, (cuuint64_t)rows, 1};
+  const cuuint64_t strides[2] = {(cuuint64_t)cols * 2, (cuuint64_t)rows * cols * 2};
   const cuuint32_t box[3] = {bx, by, 1};
   const cuuint32_t estr[3] = {1, 1, 1};
-  return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, p->d_act, dims, strides, box, estr,
+  return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, base, dims, strides, box, estr,
             CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
@@ -1594,6 +1681,7 @@ int fused_predict(mcml_mlp *p, const float *X, uint64_t n, float *mean, float *s
   const long long ctas = (long long)per_member * p->E;
   const long long scratch_rows = ctas * 2 * kFusedBatchRows;
   const long long rows_cap = std::min<long long>(kFusedRows, (long long)n);
+  const int in64 = (p->in_pad + 63) / 64 * 64;  // layer 0's contraction width
   if (!p->d_act) {
     MLP_TRY(cudaMalloc(&p->d_act, scratch_rows * p->hidden * sizeof(bf16)));
   }
@@ -1601,37 +1689,58 @@ int fused_predict(mcml_mlp *p, const float *X, uint64_t n, float *mean, float *s
     dfree(p->d_fx);
     dfree(p->d_fy);
     p->fcap = 0;
-    MLP_TRY(cudaMalloc(&p->d_fx, rows_cap * p->in_pad * sizeof(bf16)));
+    MLP_TRY(cudaMalloc(&p->d_fx, rows_cap * in64 * sizeof(bf16)));
     MLP_TRY(cudaMalloc(&p->d_fy, p->E * rows_cap * p->out_dim * sizeof(float)));
     p->fcap = rows_cap;
   }
-  CUtensorMap amap, hmap;
-  std::memset(&amap, 0, sizeof(amap));
-  std::memset(&hmap, 0, sizeof(hmap));
-  if (!encode_act_map(p, scratch_rows, 64, TCM, CU_TENSOR_MAP_SWIZZLE_128B, &amap) ||
-      !encode_act_map(p, scratch_rows, 32, 32, CU_TENSOR_MAP_SWIZZLE_64B, &hmap))
-    return set_error(MCML_E_CUDA, "mlp: tensor maps of the activation scratch");
+  // B images of the current weights
+  FusedPack pk;
+  std::memset(&pk, 0, sizeof(pk));
   FusedArgs f;
   std::memset(&f, 0, sizeof(f));
-  f.layers = p->layers;
-  f.ctas_per_member = per_member;
-  f.batch_rows = kFusedBatchRows;
-  f.hidden = p->hidden;
-  int maxKN = 0;
+  pk.layers = p->layers;
+  long long img_bytes = 0, elems = 0;
+  int maxB = 0;
   for (int l = 0; l < p->layers; ++l) {
-    f.K[l] = p->fan_in[l];
-    f.n_valid[l] = p->fan_out[l];
-    f.N[l] = (p->fan_out[l] + 15) / 16 * 16;
-    f.w_off[l] = p->w_off[l];
+    const int K = l == 0 ? in64 : p->fan_in[l];
+    const int N = (p->fan_out[l] + 15) / 16 * 16;
+    pk.K[l] = f.K[l] = K;
+    pk.N[l] = f.N[l] = N;
+    pk.fan_in[l] = p->fan_in[l];
+    pk.n_valid[l] = f.n_valid[l] = p->fan_out[l];
+    pk.w_off[l] = p->w_off[l];
+    pk.elem_begin[l] = elems;
+    pk.img_off[l] = f.img_off[l] = img_bytes;
     f.b_off[l] = p->b_off[l];
-    maxKN = std::max(maxKN, f.K[l] * f.N[l]);
+    elems += (long long)K * N;
+    img_bytes += (long long)K * N * 2;
+    maxB = std::max(maxB, K * N * 2);
   }
-  f.W = p->d_w16;
+  pk.elem_begin[p->layers] = elems;
+  if (!p->d_wimg) MLP_TRY(cudaMalloc(&p->d_wimg, p->E * img_bytes));
+  fused_pack_kernel<<<dim3((unsigned)((elems + 255) / 256), 1, p->E), 256, 0, p->stream>>>(
+      p->d_w16, p->stride, pk, p->d_wimg, img_bytes);
+  MLP_TRY(cudaGetLastError());
+  CUtensorMap xmap, amap, hmap;
+  std::memset(&xmap, 0, sizeof(xmap));
+  std::memset(&amap, 0, sizeof(amap));
+  std::memset(&hmap, 0, sizeof(hmap));
+  if (!encode_rows_map(p->d_fx, in64, p->fcap, 64, TCM, CU_TENSOR_MAP_SWIZZLE_128B, &xmap) ||
+      !encode_rows_map(p->d_act, p->hidden, scratch_rows, 64, TCM, CU_TENSOR_MAP_SWIZZLE_128B,
+                       &amap) ||
+      !encode_rows_map(p->d_act, p->hidden, scratch_rows, 32, 32, CU_TENSOR_MAP_SWIZZLE_64B, &hmap))
+    return set_error(MCML_E_CUDA, "mlp: tensor maps of the fused forward");
+  f.layers = p->layers;
+  f.batch_rows = kFusedBatchRows;
+  f.img = p->d_wimg;
+  f.img_stride = img_bytes;
   f.Wf = p->d_w;
   f.strideW = p->stride;
   f.status = p->d_status;
   f.spin = p->spin;
-  const size_t fixed = tc_align1k((size_t)maxKN * 2) + kTcStageBytes + kTcSmemFixed + 1024;
+  // weights, one staging tile per epilogue warp, three bias buffers, 58
+  // barriers, TMEM slot, 1 KB of alignment slack
+  const size_t fixed = tc_align1k((size_t)maxB) + 8 * 2048 + 3 * 256 * 4 + 58 * 8 + 16 + 1024;
   const size_t slot = tc_slot_bytes(64);
   f.slots = (int)std::min<size_t>(16, (kTcSmemMax - fixed) / slot);
   if (f.slots < 2) return set_error(MCML_E_INVALID, "mlp: layers too wide for the fused forward");
@@ -1644,15 +1753,14 @@ int fused_predict(mcml_mlp *p, const float *X, uint64_t n, float *mean, float *s
   }
   for (uint64_t r0 = 0; r0 < n; r0 += (uint64_t)rows_cap) {
     const int rows = (int)std::min<uint64_t>((uint64_t)rows_cap, n - r0);
-    gather_x_kernel<<<dim3((unsigned)(((long long)rows * p->in_pad + 255) / 256), 1, 1), 256, 0,
-                      p->stream>>>(X + r0 * p->in_dim, nullptr, rows, p->in_dim, p->in_pad,
+    gather_x_kernel<<<dim3((unsigned)(((long long)rows * in64 + 255) / 256), 1, 1), 256, 0,
+                      p->stream>>>(X + r0 * p->in_dim, nullptr, rows, p->in_dim, in64,
                                    p->d_xmean, p->d_xinv, 0, p->d_fx, 0, nullptr);
     MLP_TRY(cudaGetLastError());
     f.n = rows;
-    f.X = p->d_fx;
     f.Y = p->d_fy;
-    tc_fused_forward_kernel<<<dim3(per_member, 1, p->E), kTcWarps * 32, smem, p->stream>>>(f, amap,
-                                                                                        hmap);
+    tc_fused_forward_kernel<<<dim3(per_member, 1, p->E), kTcWarps * 32, smem, p->stream>>>(
+        f, xmap, amap, hmap);
     MLP_TRY(cudaGetLastError());
     ensemble_kernel<<<(unsigned)(((long long)rows * p->out_dim + 255) / 256), 256, 0, p->stream>>>(
         p->d_fy, (long long)rows * p->out_dim, p->E, (long long)rows * p->out_dim, p->d_tmean,
