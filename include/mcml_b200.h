@@ -351,6 +351,9 @@ int mcml_wmc_rescale(const mcml_wmc_set *set, const float *base_mua, const float
  * hidden at most 256, hidden a multiple of 16, out_dim <= hidden.  Inputs and targets are normalised with
  * mcml_mlp_set_normalization; predictions come back de-normalised with the
  * ensemble's spread.  X, T, mean and spread are DEVICE arrays.
+ * mcml_mlp_predict runs every layer of every member in one launch when the
+ * hidden width is a multiple of 64 (environment MCML_MLP_FUSED=0: layer by
+ * layer, in chunks of `chunk` rows, 0 = 131072; same results bit for bit).
  */
 typedef struct mcml_mlp_config {
   int32_t in_dim, hidden, depth, out_dim, ensemble;

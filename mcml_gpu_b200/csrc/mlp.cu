@@ -2197,18 +2197,19 @@ int mcml_mlp_train_epoch(mcml_mlp *p, const float *X, const float *T, uint64_t n
 }
 
 // Inference: X [n x in] DEVICE -> mean [n x out] and ensemble spread
-// [n x out] (DEVICE, de-normalised).  With MCML_MLP_FUSED=1 in the
-// environment, networks whose hidden width is a multiple of 64 run all
-// layers in one launch per up to 2^22 rows (fused_predict); otherwise layer
-// by layer in chunks of the activation buffers.
+// [n x out] (DEVICE, de-normalised).  Networks whose hidden width is a
+// multiple of 64 run all layers in one launch per up to 2^22 rows
+// (fused_predict; MCML_MLP_FUSED=0 in the environment turns it off); the
+// others layer by layer in chunks of `chunk` rows (0: 131072).  Both paths
+// round at the same points and give the same results bit for bit.
 int mcml_mlp_predict(mcml_mlp *p, const float *X, uint64_t n, float *mean, float *spread,
                      uint32_t chunk) {
   clear_error();
   if (!p || !X || !mean) return set_error(MCML_E_INVALID, "bad argument");
   MlpGuard gd(p->device);
   const char *fz = std::getenv("MCML_MLP_FUSED");
-  if (fused_eligible(p) && fz && fz[0] == '1') return fused_predict(p, X, n, mean, spread);
-  if (chunk == 0) chunk = 65536;
+  if (fused_eligible(p) && !(fz && fz[0] == '0')) return fused_predict(p, X, n, mean, spread);
+  if (chunk == 0) chunk = 131072;
   int rc = ensure_cap(p, (int)std::min<uint64_t>(chunk, n));
   if (rc) return rc;
   const long long cap = p->cap;

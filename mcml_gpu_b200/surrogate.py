@@ -131,8 +131,9 @@ class MLP:
                "mcml_mlp_train_epoch")
         return loss
 
-    def predict(self, X, chunk: int = 65536):
-        """X: (n, in) float32 CUDA tensor -> (mean, spread) CUDA tensors (n, out)."""
+    def predict(self, X, chunk: int = 0):
+        """X: (n, in) float32 CUDA tensor -> (mean, spread) CUDA tensors (n, out).
+        chunk: rows per step of the layer-by-layer path (0: the library default)."""
         import torch
         px = _device_ptr(X, "X", device=self.device, shape=(None, self.in_dim))
         n = X.shape[0]
