@@ -347,7 +347,7 @@ int mcml_wmc_rescale(const mcml_wmc_set *set, const float *base_mua, const float
  * library's BF16 tensor-core kernels with FP32 accumulation and FP32
  * master weights (Adam), forward and backward products on tcgen05
  * (accumulators in tensor memory; the output layer's 3-wide input
- * gradient on mma.sync).  Limits: in_dim and
+ * gradient on the CUDA cores).  Limits: in_dim and
  * hidden at most 256, hidden a multiple of 16, out_dim <= hidden.  Inputs and targets are normalised with
  * mcml_mlp_set_normalization; predictions come back de-normalised with the
  * ensemble's spread.  X, T, mean and spread are DEVICE arrays.

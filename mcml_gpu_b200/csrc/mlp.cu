@@ -13,16 +13,15 @@
 // Backward: the hidden layers' dH = (dZ W^T) * gelu'(Z) on tc_layer_kernel
 // (weights as a K-major B operand) and the weight gradients dW = X^T dZ
 // (X as an MN-major A operand, 256-row batch slices added atomically); the
-// output layer's 3-wide dH, and dW of batches that are not whole slices,
-// on the GEMM below.
+// output layer's 3-wide dH on the CUDA cores (narrow_back_kernel); dW of
+// batches that are not whole 256-row slices on the GEMM below.
 //
 // Backward GEMM: C[M x N] = op(A)[M x K] * op(B)[K x N], BF16 operands staged in
 // shared memory, mma.sync m16n8k16 fragments loaded with ldmatrix, FP32
 // accumulators, and a fused epilogue:
 //   kGeluBack : dZ = bf16(acc * gelu'(Zprev))   (back through an activation)
 //   kStoreF32 : G = acc (FP32; weight gradients)
-// op(A) = A or A^T, op(B) = B or B^T by template flags, which gives the
-// backward products dW = H^T dZ and dH = dZ W^T from the same kernel.
+// op(A) = A or A^T, op(B) = B or B^T by template flags.
 #include <cuda.h>  // CUtensorMap (the encoder is reached through the runtime)
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -1413,6 +1412,26 @@ __global__ void bias_grad_kernel(const bf16 *dZ, long long strideD, int n, int c
   atomicAdd(&db[z * strideB + c], s);
 }
 
+// dH = (dZ W^T) * gelu'(Z) of a layer whose fan-out fo is not a multiple
+// of 16 (the output layer): fo FP32 multiply-adds of the BF16 operands per
+// element, in order, then the GELU derivative and one rounding to BF16 --
+// the tensor-core kernel's arithmetic for a K this narrow.
+__global__ void narrow_back_kernel(const bf16 *dZ, int ld_dz, long long stride_dz, const bf16 *W,
+                                   long long strideW, int fo, const float *Z, int ldz,
+                                   long long strideZ, bf16 *dH, int ldh, long long strideH, int n,
+                                   int fi) {
+  const int zm = blockIdx.z;
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (long long)n * fi) return;
+  const int r = (int)(e / fi), j = (int)(e % fi);
+  const bf16 *dz = dZ + zm * stride_dz + (long long)r * ld_dz;
+  const bf16 *w = W + zm * strideW + (long long)j * fo;
+  float acc = 0.0f;
+  for (int o = 0; o < fo; ++o) acc = fmaf(__bfloat162float(dz[o]), __bfloat162float(w[o]), acc);
+  const float zz = Z[zm * strideZ + (long long)r * ldz + j];
+  dH[zm * strideH + (long long)r * ldh + j] = __float2bfloat16(acc * gelu_grad(zz));
+}
+
 // Adam on the FP32 master weights; refreshes the BF16 mirror.
 // Adam step number st->t + 1 with learning rate st->lr.
 __global__ void adam_kernel(float *w, const float *grad, float *m, float *v, bf16 *w16,
@@ -1847,7 +1866,8 @@ int backward(mcml_mlp *p, int n) {
     if (l == 0) break;
     // dZ_{l-1} = (dZ_l W_l^T) * gelu'(Z_{l-1})   (M = n, N = fi, K = fo):
     // on the tensor cores (W_l as a K-major B operand) when fo is a hidden
-    // width; the output layer's narrow fo stays on the mma.sync kernel
+    // width; the output layer's narrow fo (3 multiply-adds per element) on
+    // the CUDA cores
     if (fo % 16 == 0) {
       TcArgs t;
       std::memset(&t, 0, sizeof(t));
@@ -1873,24 +1893,12 @@ int backward(mcml_mlp *p, int n) {
       dcur_ld = H;
       continue;
     }
-    GemmArgs b;
-    std::memset(&b, 0, sizeof(b));
-    b.M = n;
-    b.N = fi;
-    b.K = fo;
-    b.A = dcur;
-    b.lda = dcur_ld;
-    b.strideA = cap * std::max<long long>(H, p->out_dim);
-    b.B = p->d_w16 + p->w_off[l];
-    b.ldb = fo;
-    b.strideB = P;
-    b.outH = dnext;
-    b.ldh = H;
-    b.strideH = cap * std::max<long long>(H, p->out_dim);
-    b.aux = p->d_z + (long long)(l - 1) * cap * H;
-    b.ldx = H;
-    b.strideX = D * cap * H;
-    MLP_TRY((gemm<false, true, kGeluBack>(b, p->E, p->stream)));
+    narrow_back_kernel<<<dim3((unsigned)(((long long)n * fi + 255) / 256), 1, p->E), 256, 0,
+                         p->stream>>>(dcur, dcur_ld, cap * std::max<long long>(H, p->out_dim),
+                                      p->d_w16 + p->w_off[l], P, fo,
+                                      p->d_z + (long long)(l - 1) * cap * H, (int)H, D * cap * H,
+                                      dnext, (int)H, cap * std::max<long long>(H, p->out_dim), n, fi);
+    MLP_TRY(cudaGetLastError());
     std::swap(dcur, dnext);
     dcur_ld = H;
   }
