@@ -787,7 +787,7 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1)
 // (layer 0: the normalised inputs, padded to 64 columns; later layers: the
 // scratch) streams in by TMA in 64-column chunks, 128-byte swizzled.
 //
-// Roles (12 warps), all running through the same sequence of passes with
+// Roles (20 warps), all running through the same sequence of passes with
 // no block-wide barrier between passes:
 //  * warp 0, lane 0 -- A producer: chunk loads into a ring of shared-memory
 //    slots (a_full / a_empty).  Before loading tile t of layer l > 0 it
@@ -799,9 +799,10 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1)
 //    MMAs have completed (mma_done) brings the next pass's weights in with
 //    bulk copies of their packed image -- while the epilogue still works on
 //    the pass's last tile.
-//  * warps 4-11 -- epilogue: bias + GELU into 64-byte-swizzled staging
-//    tiles written out by TMA stores (hidden layers), or bias into FP32
-//    rows of Y (the output layer).  The epilogue threads copy each pass's
+//  * warps 4-19 -- epilogue, four warps per TMEM lane quarter, each taking
+//    every fourth 32-column chunk: bias + GELU into a 64-byte-swizzled
+//    staging tile written out by TMA stores (hidden layers), or bias into
+//    FP32 rows of Y (the output layer).  The epilogue threads copy each pass's
 //    bias into one of three shared-memory buffers (bias_ready): the
 //    double-buffered accumulators keep the slowest epilogue thread within
 //    two tiles, so within two passes, of the fastest.
@@ -811,6 +812,8 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1)
 // copies and MMAs before it frees tensor memory.
 constexpr int kMaxFusedLayers = 12;
 constexpr int kFusedMaxTiles = 16;  // batch_rows / 128
+constexpr int kFusedEpiWarps = 16;  // warps 4..19
+constexpr int kFusedWarps = 4 + kFusedEpiWarps;
 
 struct FusedArgs {
   int n;                // rows
@@ -841,7 +844,7 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t
       : "memory");
 }
 
-__global__ void __launch_bounds__(kTcWarps * 32, 1)
+__global__ void __launch_bounds__(kFusedWarps * 32, 1)
     tc_fused_forward_kernel(const FusedArgs f, const __grid_constant__ CUtensorMap tmX,
                             const __grid_constant__ CUtensorMap tmA,
                             const __grid_constant__ CUtensorMap tmH) {
@@ -856,7 +859,7 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1)
   unsigned char *sB = smem;
   unsigned char *sA = smem + (((size_t)maxB + 1023) & ~(size_t)1023);
   unsigned char *sStage = sA + (size_t)nslots * kSlot;
-  float *sBias = reinterpret_cast<float *>(sStage + (size_t)8 * 2048);  // [3][256]
+  float *sBias = reinterpret_cast<float *>(sStage + (size_t)kFusedEpiWarps * 2048);  // [3][256]
   uint64_t *bars = reinterpret_cast<uint64_t *>(sBias + 3 * 256);
   uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 58);
   const uint32_t sA_u = smem_u32(sA), sB_u = smem_u32(sB), bars_u = smem_u32(bars);
@@ -878,12 +881,12 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1)
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(acc_full(b), 1);
-      mbar_init(acc_empty(b), 256);
+      mbar_init(acc_empty(b), kFusedEpiWarps * 32);
     }
     mbar_init(w_full, 1);
     mbar_init(mma_done, 1);
-    for (int t = 0; t < kFusedMaxTiles; ++t) mbar_init(h_done(t), 8);
-    for (int i = 0; i < 3; ++i) mbar_init(bias_ready(i), 256);
+    for (int t = 0; t < kFusedMaxTiles; ++t) mbar_init(h_done(t), kFusedEpiWarps);
+    for (int i = 0; i < 3; ++i) mbar_init(bias_ready(i), kFusedEpiWarps * 32);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   if (warp == 0) {  // two 256-column accumulators: all of tensor memory
@@ -1063,8 +1066,9 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1)
     }
     __syncwarp();
   } else if (warp >= 4) {
-    // ---- epilogue: warp w drains TMEM lanes 32*(w%4).., column half (w-4)/4
-    const int q = warp & 3, half = (warp - 4) >> 2;
+    // ---- epilogue: warp w drains TMEM lanes 32*(w%4).. (the lanes it may
+    // access) and the 32-column chunks part, part+4, ... of them
+    const int q = warp & 3, part = (warp - 4) >> 2;
     unsigned char *my_stage = sStage + (warp - 4) * 2048;  // one staging tile per warp
     int pend = -1;    // lane 0: tile whose stores are issued but not yet signalled
     auto signal_stored = [&]() {
@@ -1084,13 +1088,12 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1)
       pass_rows(wp, r0, tiles);
       const int N = f.N[l], nv = f.n_valid[l];
       const int rows = min(BR, f.n - r0);
-      const int c_begin = half * (N / 2);
       const int h_row0 = (cta * 2 + (l & 1)) * BR;
       // this pass's bias into buffer wp % 3, completed on bias_ready
       float *bias = sBias + (wp % 3) * 256;
       {
-        const int e = tid - 128;  // 0..255
-        bias[e] = e < nv ? f.Wf[(long long)z * f.strideW + f.b_off[l] + e] : 0.0f;
+        const int e = tid - 128;  // 0..511
+        if (e < 256) bias[e] = e < nv ? f.Wf[(long long)z * f.strideW + f.b_off[l] + e] : 0.0f;
         mbar_arrive(bias_ready(wp % 3));
         if (s_err || !mbar_wait(bias_ready(wp % 3), (uint32_t)((wp / 3) & 1), f.spin)) {
           atomicOr(f.status, 1u);
@@ -1133,24 +1136,18 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1)
               asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
             }
           };
-          uint32_t va[32], vb[32];
-          tmem_ld32(va, tbase + c_begin);
-          tmem_wait();
-          for (int c = 0; c < chunks; c += 2) {
-            if (c + 1 < chunks) tmem_ld32(vb, tbase + c_begin + (c + 1) * 32);
-            emit(va, c_begin + c * 32);
+          (void)chunks;
+          uint32_t va[32];
+          for (int c = part; c < N / 32; c += 4) {
+            tmem_ld32(va, tbase + c * 32);
             tmem_wait();
-            if (c + 1 < chunks) {
-              if (c + 2 < chunks) tmem_ld32(va, tbase + c_begin + (c + 2) * 32);
-              emit(vb, c_begin + (c + 1) * 32);
-              tmem_wait();
-            }
+            emit(va, c * 32);
           }
           pend = t;
         } else {
           // output layer: bias -> FP32 rows of Y (real columns, real rows)
           const int grow = r0 + lrow;
-          for (int c0 = c_begin; c0 < c_begin + N / 2; c0 += 8) {
+          for (int c0 = part * 8; c0 < N; c0 += 32) {
             uint32_t v[8];
             asm volatile(
                 "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
@@ -1759,7 +1756,8 @@ int fused_predict(mcml_mlp *p, const float *X, uint64_t n, float *mean, float *s
   f.spin = p->spin;
   // weights, one staging tile per epilogue warp, three bias buffers, 58
   // barriers, TMEM slot, 1 KB of alignment slack
-  const size_t fixed = tc_align1k((size_t)maxB) + 8 * 2048 + 3 * 256 * 4 + 58 * 8 + 16 + 1024;
+  const size_t fixed =
+      tc_align1k((size_t)maxB) + kFusedEpiWarps * 2048 + 3 * 256 * 4 + 58 * 8 + 16 + 1024;
   const size_t slot = tc_slot_bytes(64);
   f.slots = (int)std::min<size_t>(16, (kTcSmemMax - fixed) / slot);
   if (f.slots < 2) return set_error(MCML_E_INVALID, "mlp: layers too wide for the fused forward");
@@ -1778,7 +1776,7 @@ int fused_predict(mcml_mlp *p, const float *X, uint64_t n, float *mean, float *s
     MLP_TRY(cudaGetLastError());
     f.n = rows;
     f.Y = p->d_fy;
-    tc_fused_forward_kernel<<<dim3(per_member, 1, p->E), kTcWarps * 32, smem, p->stream>>>(
+    tc_fused_forward_kernel<<<dim3(per_member, 1, p->E), kFusedWarps * 32, smem, p->stream>>>(
         f, xmap, amap, hmap);
     MLP_TRY(cudaGetLastError());
     ensemble_kernel<<<(unsigned)(((long long)rows * p->out_dim + 255) / 256), 256, 0, p->stream>>>(
