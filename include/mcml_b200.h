@@ -352,8 +352,9 @@ int mcml_wmc_rescale(const mcml_wmc_set *set, const float *base_mua, const float
  * mcml_mlp_set_normalization; predictions come back de-normalised with the
  * ensemble's spread.  X, T, mean and spread are DEVICE arrays.
  * mcml_mlp_predict runs every layer of every member in one launch when the
- * hidden width is a multiple of 64 (environment MCML_MLP_FUSED=0: layer by
- * layer, in chunks of `chunk` rows, 0 = 131072; same results bit for bit).
+ * hidden width is a multiple of 64 and out_dim <= 3 (environment
+ * MCML_MLP_FUSED=0: layer by layer, in chunks of `chunk` rows, 0 = 131072;
+ * the two differ only in the order of the output layer's FP32 sums).
  */
 typedef struct mcml_mlp_config {
   int32_t in_dim, hidden, depth, out_dim, ensemble;

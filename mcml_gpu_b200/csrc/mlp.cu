@@ -781,14 +781,19 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1)
 // Whole-network forward for inference on the tensor cores: every layer of
 // every member in one launch.  CTA (c, member z) takes batches of
 // batch_rows rows (whole 128-row tiles) and runs each batch through all the
-// layers before the next batch.  A (batch, layer) pair is a *pass*.  The
+// layers before the next batch.  The hidden layers run on the tensor cores,
+// one *pass* per (batch, layer); the output layer (at most kFusedMaxOut
+// columns) is folded into the last hidden layer's epilogue, which rounds
+// that layer's activations to BF16 as a store would and multiplies them by
+// the output weights on the CUDA cores, so no pass loads them back.  The
 // batch's activations pass between layers through the CTA's own
 // batch_rows scratch rows, written in place: a layer's epilogue stores
 // tile t only after that tile's MMAs -- and so its loads of tile t -- have
 // completed, and the next layer loads tile t only after those stores have
 // (h_done).  One buffer per CTA keeps the whole scratch (148 x 1024 rows x
 // 512 bytes at width 256) inside L2; two buffers did not fit and measured
-// 3.36 against 3.00 ms for 1e6 queries x 4 members.  Every A operand
+// 3.36 against 3.00 ms for 1e6 queries x 4 members (the folded output
+// layer then took it to 2.62 ms).  Every A operand
 // (layer 0: the normalised inputs, padded to 64 columns; later layers: the
 // scratch) streams in by TMA in 64-column chunks, 128-byte swizzled.
 //
@@ -806,8 +811,10 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1)
 //    the pass's last tile.
 //  * warps 4-19 -- epilogue, four warps per TMEM lane quarter, each taking
 //    every fourth 32-column chunk: bias + GELU into a 64-byte-swizzled
-//    staging tile written out by TMA stores (hidden layers), or bias into
-//    FP32 rows of Y (the output layer).  The epilogue threads copy each pass's
+//    staging tile written out by TMA stores; in the last pass bias + GELU
+//    + BF16 rounding times the output weights, the four warps' partial
+//    sums of a row added in a fixed order through shared memory (sRed,
+//    red_bar) into the FP32 rows of Y.  The epilogue threads copy each pass's
 //    bias into one of three shared-memory buffers (bias_ready): the
 //    double-buffered accumulators keep the slowest epilogue thread within
 //    two tiles, so within two passes, of the fastest.
@@ -818,6 +825,7 @@ __global__ void __launch_bounds__(kTcWarps * 32, 1)
 constexpr int kMaxFusedLayers = 12;
 constexpr int kFusedMaxTiles = 16;  // batch_rows / 128
 constexpr int kFusedEpiWarps = 16;  // warps 4..19
+constexpr int kFusedMaxOut = 3;     // output columns folded into the last hidden epilogue
 constexpr int kFusedWarps = 4 + kFusedEpiWarps;
 
 struct FusedArgs {
@@ -834,6 +842,9 @@ struct FusedArgs {
   const float *Wf;                // FP32 parameters (the biases); member z at z * strideW
   long long strideW;
   float *Y;                       // members x n x n_valid[last]
+  const bf16 *W16;                // BF16 parameters (the output layer's weights); member z at z * strideW
+  long long w_off_out, b_off_out; // the output layer's weights and bias
+  int out_dim;                    // at most kFusedMaxOut
   int slots;                      // A ring slots
   unsigned *status;
   long long spin;
@@ -847,6 +858,29 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t
           dst),
       "l"(src), "r"(bytes), "r"(bar)
       : "memory");
+}
+
+// Bias + GELU of 32 accumulator columns [c0, c0+32) of one row, rounded to
+// BF16 like a stored activation, then folded into the output layer:
+// acc[o] += h_c * Wout[c][o] in column order.
+__device__ __forceinline__ void fused_gelu_fold32(const uint32_t (&v)[32], int c0,
+                                                  const float *bias, const float4 *wo,
+                                                  float (&acc)[kFusedMaxOut]) {
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    const float2 b = *reinterpret_cast<const float2 *>(bias + c0 + 2 * i);
+    const float2 g2 = gelu2(
+        __fadd2_rn(make_float2(__uint_as_float(v[2 * i]), __uint_as_float(v[2 * i + 1])), b));
+    const __nv_bfloat162 h = __floats2bfloat162_rn(g2.x, g2.y);
+    const float hx = __low2float(h), hy = __high2float(h);
+    const float4 w0 = wo[c0 + 2 * i], w1 = wo[c0 + 2 * i + 1];
+    acc[0] = fmaf(hx, w0.x, acc[0]);
+    acc[1] = fmaf(hx, w0.y, acc[1]);
+    acc[2] = fmaf(hx, w0.z, acc[2]);
+    acc[0] = fmaf(hy, w1.x, acc[0]);
+    acc[1] = fmaf(hy, w1.y, acc[1]);
+    acc[2] = fmaf(hy, w1.z, acc[2]);
+  }
 }
 
 __global__ void __launch_bounds__(kFusedWarps * 32, 1)
@@ -865,8 +899,10 @@ __global__ void __launch_bounds__(kFusedWarps * 32, 1)
   unsigned char *sA = smem + (((size_t)maxB + 1023) & ~(size_t)1023);
   unsigned char *sStage = sA + (size_t)nslots * kSlot;
   float *sBias = reinterpret_cast<float *>(sStage + (size_t)kFusedEpiWarps * 2048);  // [3][256]
-  uint64_t *bars = reinterpret_cast<uint64_t *>(sBias + 3 * 256);
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 58);
+  float4 *sWo = reinterpret_cast<float4 *>(sBias + 3 * 256);  // [256]: output weights, FP32
+  float *sRed = reinterpret_cast<float *>(sWo + 256);          // [2][3][128][3] partial outputs
+  uint64_t *bars = reinterpret_cast<uint64_t *>(sRed + 2 * 3 * 128 * 3);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 60);
   const uint32_t sA_u = smem_u32(sA), sB_u = smem_u32(sB), bars_u = smem_u32(bars);
   auto a_full = [&](int s) { return bars_u + 8u * s; };
   auto a_empty = [&](int s) { return bars_u + 8u * (16 + s); };
@@ -876,6 +912,7 @@ __global__ void __launch_bounds__(kFusedWarps * 32, 1)
   const uint32_t mma_done = bars_u + 8u * 37;
   auto h_done = [&](int t) { return bars_u + 8u * (38 + t); };
   auto bias_ready = [&](int i) { return bars_u + 8u * (54 + i); };  // 3 of the 4 used
+  auto red_bar = [&](int i) { return bars_u + 8u * (58 + i); };
   volatile int &s_err = *reinterpret_cast<volatile int *>(tslot + 1);
 
   if (tid == 0) {
@@ -892,7 +929,18 @@ __global__ void __launch_bounds__(kFusedWarps * 32, 1)
     mbar_init(mma_done, 1);
     for (int t = 0; t < kFusedMaxTiles; ++t) mbar_init(h_done(t), kFusedEpiWarps);
     for (int i = 0; i < 3; ++i) mbar_init(bias_ready(i), kFusedEpiWarps * 32);
+    for (int i = 0; i < 2; ++i) mbar_init(red_bar(i), kFusedEpiWarps * 32);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  {
+    // the output layer's weights (BF16 values, held as FP32)
+    const int H = f.K[f.layers - 1];
+    const bf16 *wo = f.W16 + (long long)z * f.strideW + f.w_off_out;
+    for (int k = tid; k < H; k += kFusedWarps * 32) {
+      float w[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+      for (int o = 0; o < f.out_dim; ++o) w[o] = __bfloat162float(wo[(long long)k * f.out_dim + o]);
+      sWo[k] = make_float4(w[0], w[1], w[2], w[3]);
+    }
   }
   if (warp == 0) {  // two 256-column accumulators: all of tensor memory
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
@@ -912,11 +960,14 @@ __global__ void __launch_bounds__(kFusedWarps * 32, 1)
   const int nb = (int)blockIdx.x < batches
                      ? (batches - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x
                      : 0;
-  const int passes = nb * L;
+  // the layers that run on the tensor cores; the output layer is folded
+  // into the last one's epilogue
+  const int LP = L - 1;
+  const int passes = nb * LP;
   const int cta = z * gridDim.x + blockIdx.x;
   // the rows and tiles of pass wp's batch
   auto pass_rows = [&](int wp, int &r0, int &tiles) {
-    const int bt = (int)blockIdx.x + (wp / L) * (int)gridDim.x;
+    const int bt = (int)blockIdx.x + (wp / LP) * (int)gridDim.x;
     r0 = bt * BR;
     const int rows = min(BR, f.n - r0);
     tiles = (rows + TCM - 1) / TCM;
@@ -928,7 +979,7 @@ __global__ void __launch_bounds__(kFusedWarps * 32, 1)
       int gi = 0;  // chunk sequence number over all passes
       bool alive = true;
       for (int wp = 0; wp < passes && alive; ++wp) {
-        const int j = wp / L, l = wp % L;
+        const int j = wp / LP, l = wp % LP;
         int r0, tiles;
         pass_rows(wp, r0, tiles);
         const int nch = f.K[l] / 64;
@@ -936,8 +987,8 @@ __global__ void __launch_bounds__(kFusedWarps * 32, 1)
         for (int t = 0; t < tiles && alive; ++t) {
           if (l > 0) {
             // layer l-1's stores of this tile are complete (completion
-            // number j*(L-1) + l-1 of h_done[t]: one per hidden layer and batch)
-            if (s_err || !mbar_wait(h_done(t), (uint32_t)((j * (L - 1) + l - 1) & 1), f.spin)) {
+            // number j*(LP-1) + l-1 of h_done[t]: one per stored layer and batch)
+            if (s_err || !mbar_wait(h_done(t), (uint32_t)((j * (LP - 1) + l - 1) & 1), f.spin)) {
               atomicOr(f.status, 1u);
               s_err = 1;
               alive = false;
@@ -985,7 +1036,7 @@ __global__ void __launch_bounds__(kFusedWarps * 32, 1)
     if (lane == 0) {
       const unsigned char *img = f.img + (long long)z * f.img_stride;
       auto load_weights = [&](int wp) {
-        const int l = wp % L;
+        const int l = wp % LP;
         const uint32_t bytes = (uint32_t)(f.K[l] * f.N[l] * 2);
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(w_full),
                      "r"(bytes)
@@ -1001,7 +1052,7 @@ __global__ void __launch_bounds__(kFusedWarps * 32, 1)
       }
       bool alive = true;
       for (int wp = 0; wp < passes && alive; ++wp) {
-        const int l = wp % L;
+        const int l = wp % LP;
         int r0, tiles;
         pass_rows(wp, r0, tiles);
         (void)r0;
@@ -1085,10 +1136,11 @@ __global__ void __launch_bounds__(kFusedWarps * 32, 1)
       }
     };
     int tseq = 0;
+    int otile = 0;  // tiles of the last pass so far (sRed / red_bar buffer and phase)
     bool alive = true;
     for (int wp = 0; wp < passes && alive; ++wp) {
-      const int l = wp % L;
-      const bool last = l == L - 1;
+      const int l = wp % LP;
+      const bool last = l == LP - 1;
       int r0, tiles;
       pass_rows(wp, r0, tiles);
       const int N = f.N[l], nv = f.n_valid[l];
@@ -1150,22 +1202,42 @@ __global__ void __launch_bounds__(kFusedWarps * 32, 1)
           }
           pend = t;
         } else {
-          // output layer: bias -> FP32 rows of Y (real columns, real rows)
-          const int grow = r0 + lrow;
-          for (int c0 = part * 8; c0 < N; c0 += 32) {
-            uint32_t v[8];
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
-                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
-                  "=r"(v[6]), "=r"(v[7])
-                : "r"(tbase + (uint32_t)c0));
+          // last tensor-core layer: bias + GELU + BF16 rounding folded into
+          // the output layer; the four warps of a lane quarter add their
+          // partial sums in part order through sRed, and part 0 writes Y
+          float acc[kFusedMaxOut] = {0.0f, 0.0f, 0.0f};
+          uint32_t va[32];
+          for (int c = part; c < N / 32; c += 4) {
+            tmem_ld32(va, tbase + c * 32);
             tmem_wait();
-            if (lrow >= rows) continue;
-            float *y = f.Y + ((long long)z * f.n + grow) * nv;
-#pragma unroll
-            for (int i = 0; i < 8; ++i)
-              if (c0 + i < nv) y[c0 + i] = __uint_as_float(v[i]) + bias[c0 + i];
+            fused_gelu_fold32(va, c * 32, bias, sWo, acc);
           }
+          const int ob = otile & 1;
+          const int row = q * 32 + lane;
+          if (part > 0) {
+            float *r = sRed + (((ob * 3) + part - 1) * 128 + row) * 3;
+            r[0] = acc[0];
+            r[1] = acc[1];
+            r[2] = acc[2];
+          }
+          mbar_arrive(red_bar(ob));
+          if (part == 0) {
+            if (s_err || !mbar_wait(red_bar(ob), (uint32_t)((otile >> 1) & 1), f.spin)) {
+              atomicOr(f.status, 1u);
+              s_err = 1;
+            } else if (lrow < rows) {
+              float *y = f.Y + ((long long)z * f.n + r0 + lrow) * f.out_dim;
+              const float *bo = f.Wf + (long long)z * f.strideW + f.b_off_out;
+#pragma unroll
+              for (int o = 0; o < kFusedMaxOut; ++o) {
+                float sum = acc[o];
+#pragma unroll
+                for (int pp = 0; pp < 3; ++pp) sum += sRed[(((ob * 3) + pp) * 128 + row) * 3 + o];
+                if (o < f.out_dim) y[o] = sum + bo[o];
+              }
+            }
+          }
+          ++otile;
         }
         asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
         mbar_arrive(acc_empty(b));
@@ -1666,10 +1738,13 @@ int check_status(mcml_mlp *p) {
 // Whole-network inference (tc_fused_forward_kernel) applies when every
 // hidden layer can stream its activations by TMA and store them in 32-column
 // TMA tiles: hidden width a multiple of 64, at most kMaxFusedLayers layers,
-// an output of at most 16 columns, hidden biases at 8-byte-aligned offsets.
+// an output of at most kFusedMaxOut columns, hidden biases at 8-byte-aligned
+// offsets.  Its results differ from the layer kernel's only by the order in
+// which the output layer's FP32 sums are added (a few units in the last
+// place).
 bool fused_eligible(const mcml_mlp *p) {
   if (!(p->hidden % 64 == 0 && p->hidden <= 256 && p->layers <= kMaxFusedLayers &&
-        p->out_dim <= 16 && p->in_pad <= 256))
+        p->layers >= 2 && p->out_dim <= kFusedMaxOut && p->in_pad <= 256))
     return false;
   for (int l = 0; l + 1 < p->layers; ++l)
     if (p->b_off[l] % 2) return false;
@@ -1754,6 +1829,10 @@ int fused_predict(mcml_mlp *p, const float *X, uint64_t n, float *mean, float *s
   f.layers = p->layers;
   f.batch_rows = kFusedBatchRows;
   f.img = p->d_wimg;
+  f.W16 = p->d_w16;
+  f.w_off_out = p->w_off[p->layers - 1];
+  f.b_off_out = p->b_off[p->layers - 1];
+  f.out_dim = p->out_dim;
   f.img_stride = img_bytes;
   f.Wf = p->d_w;
   f.strideW = p->stride;
@@ -1762,7 +1841,8 @@ int fused_predict(mcml_mlp *p, const float *X, uint64_t n, float *mean, float *s
   // weights, one staging tile per epilogue warp, three bias buffers, 58
   // barriers, TMEM slot, 1 KB of alignment slack
   const size_t fixed =
-      tc_align1k((size_t)maxB) + kFusedEpiWarps * 2048 + 3 * 256 * 4 + 58 * 8 + 16 + 1024;
+      tc_align1k((size_t)maxB) + kFusedEpiWarps * 2048 + 3 * 256 * 4 + 256 * 16 +
+      2 * 3 * 128 * 3 * 4 + 60 * 8 + 16 + 1024;
   const size_t slot = tc_slot_bytes(64);
   f.slots = (int)std::min<size_t>(16, (kTcSmemMax - fixed) / slot);
   if (f.slots < 2) return set_error(MCML_E_INVALID, "mlp: layers too wide for the fused forward");
@@ -2209,10 +2289,11 @@ int mcml_mlp_train_epoch(mcml_mlp *p, const float *X, const float *T, uint64_t n
 
 // Inference: X [n x in] DEVICE -> mean [n x out] and ensemble spread
 // [n x out] (DEVICE, de-normalised).  Networks whose hidden width is a
-// multiple of 64 run all layers in one launch per up to 2^22 rows
-// (fused_predict; MCML_MLP_FUSED=0 in the environment turns it off); the
-// others layer by layer in chunks of `chunk` rows (0: 131072).  Both paths
-// round at the same points and give the same results bit for bit.
+// multiple of 64 and whose output has at most 3 columns run all layers in
+// one launch per up to 2^22 rows (fused_predict; MCML_MLP_FUSED=0 in the
+// environment turns it off); the others layer by layer in chunks of
+// `chunk` rows (0: 131072).  Both paths round at the same points; they
+// differ only in the order of the output layer's FP32 additions.
 int mcml_mlp_predict(mcml_mlp *p, const float *X, uint64_t n, float *mean, float *spread,
                      uint32_t chunk) {
   clear_error();

@@ -199,14 +199,18 @@ def test_pipeline_wait_timeout_is_reported_and_drained(gpu_available, monkeypatc
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("hidden,depth,n", [(256, 4, 3000), (64, 3, 1000), (128, 2, 70000)])
-def test_fused_forward_equals_layer_by_layer(hidden, depth, n, gpu_available, monkeypatch):
+@pytest.mark.parametrize("hidden,depth,n", [(256, 4, 3000), (64, 3, 1000), (128, 2, 70000),
+                                            (256, 1, 5000)])  # depth 1: the output folded into layer 0
+def test_fused_forward_agrees_with_layer_by_layer(hidden, depth, n, gpu_available, monkeypatch):
     """With a hidden width that is a multiple of 64 and MCML_MLP_FUSED=1,
     predict() runs every layer of every member in one launch (the fused
-    kernel, activations kept in each CTA's L2-resident scratch); without it,
-    one launch per layer.  Both round to BF16 at the same points and issue
-    the same tensor-core MMAs in the same order, so they agree bit for bit --
-    including a last batch of rows that is not a whole 512-row batch."""
+    kernel, activations kept in each CTA's L2-resident scratch, the output
+    layer folded into the last hidden layer's epilogue); without it, one
+    launch per layer.  Both round to BF16 at the same points and issue the
+    same tensor-core MMAs for the hidden layers; the output layer's FP32 sums
+    are added in another order, so the two agree to a few units in the last
+    place of the output scale -- also for a last batch of rows that is not a
+    whole 1024-row batch."""
     rng = np.random.default_rng(13)
     X = torch.from_numpy(rng.normal(size=(n, 25)).astype(np.float32)).cuda()
     mlp = sg.MLP(25, 3, hidden=hidden, depth=depth, ensemble=4, seed=21)
@@ -224,5 +228,5 @@ def test_fused_forward_equals_layer_by_layer(hidden, depth, n, gpu_available, mo
     err_f = float(np.max(np.abs(fm.cpu().numpy() - ys.mean(0))))
     err_l = float(np.max(np.abs(lm.cpu().numpy() - ys.mean(0))))
     assert err_f < 1e-2 * scale and err_l < 1e-2 * scale, (err_f, err_l, scale)
-    assert torch.equal(fm, lm), float((fm - lm).abs().max())
-    assert torch.equal(fs, ls)
+    assert float((fm - lm).abs().max()) <= 1e-5 * scale, float((fm - lm).abs().max())
+    assert float((fs - ls).abs().max()) <= 1e-4 * scale, float((fs - ls).abs().max())
