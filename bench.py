@@ -575,7 +575,7 @@ def surrogate_arm(args) -> int:
         X[i, 5 * l + which] = (rng.uniform(lo - ext, lo) if rng.random() < 0.5
                                else rng.uniform(hi, hi + ext))
     Xt = torch.from_numpy(X).cuda()
-    sur.mlp.predict(Xt[:65536])  # warm-up
+    sur.mlp.predict(Xt)  # warm-up at the full size (buffers sized once, outside the timing)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     mean, spread = sur.mlp.predict(Xt)
