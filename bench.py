@@ -555,9 +555,16 @@ def surrogate_arm(args) -> int:
     label_s = time.perf_counter() - t0
     t0 = time.perf_counter()
     fb_photons = int(args.fallback_photons)
-    sur = sg.Surrogate.train(labels, epochs=args.epochs, batch=4096, lr=2e-3, seed=1,
-                             max_spread=0.05, fallback_photons=fb_photons)
+    sur = sg.Surrogate.train(labels, epochs=args.epochs, batch=args.train_batch,
+                             lr=args.train_lr, seed=1, max_spread=0.05,
+                             fallback_photons=fb_photons)
     train_s = time.perf_counter() - t0
+    # training FLOPs: forward + input and weight gradients (3 x the forward's
+    # 2 x multiply-adds of the real widths) for every row of every full
+    # minibatch, 4 members
+    macs = 25 * 256 + 3 * 256 * 256 + 256 * 3
+    n_lab = int(labels.X.shape[0])
+    train_flop = 3 * 2.0 * macs * 4 * (n_lab // args.train_batch * args.train_batch) * args.epochs
     rng = np.random.default_rng(5)
     # 1e6 queries: mua and mus of every layer uniform over the tissue's ranges;
     # 5 % of them take one coefficient from the 20 %-widened ranges' excess,
@@ -692,7 +699,8 @@ def surrogate_arm(args) -> int:
         "labels": {"count": int(labels.X.shape[0]), "baselines": args.baselines,
                    "photons_per_baseline": int(args.label_photons), "seconds": label_s,
                    "mua_baseline": args.label_mua_baseline, "mus_jitter": args.label_mus_jitter},
-        "training": {"epochs": args.epochs, "seconds": train_s,
+        "training": {"epochs": args.epochs, "seconds": train_s, "batch": args.train_batch,
+                     "lr": args.train_lr, "tflops": train_flop / train_s / 1e12,
                      "final_loss": [float(v) for v in sur.history[-1]]},
         "config": {"workload": "surrogate: WMC labels, MLP 25->256x4->3 GELU, ensemble 4, "
                                "BF16 tensor-core kernels; ring detectors 0.5/1.0/1.5 cm",
@@ -899,6 +907,8 @@ def main() -> int:
     ap.add_argument("--label-mus-jitter", type=float, default=0.05)
     ap.add_argument("--combos", type=int, default=2_000_000)
     ap.add_argument("--epochs", type=int, default=20)
+    ap.add_argument("--train-batch", type=int, default=8192)
+    ap.add_argument("--train-lr", type=float, default=2.8e-3)
     ap.add_argument("--queries", type=int, default=1_000_000)
     ap.add_argument("--heldout", type=int, default=1000)
     ap.add_argument("--heldout-out", type=int, default=40,
