@@ -827,6 +827,7 @@ constexpr int kFusedMaxTiles = 16;  // batch_rows / 128
 constexpr int kFusedEpiWarps = 16;  // warps 4..19
 constexpr int kFusedMaxOut = 3;     // output columns folded into the last hidden epilogue
 constexpr int kFusedWarps = 4 + kFusedEpiWarps;
+constexpr int kFusedParts = kFusedEpiWarps / 4;  // epilogue warps per TMEM lane quarter
 
 struct FusedArgs {
   int n;                // rows
@@ -900,8 +901,8 @@ __global__ void __launch_bounds__(kFusedWarps * 32, 1)
   unsigned char *sStage = sA + (size_t)nslots * kSlot;
   float *sBias = reinterpret_cast<float *>(sStage + (size_t)kFusedEpiWarps * 2048);  // [3][256]
   float4 *sWo = reinterpret_cast<float4 *>(sBias + 3 * 256);  // [256]: output weights, FP32
-  float *sRed = reinterpret_cast<float *>(sWo + 256);          // [2][3][128][3] partial outputs
-  uint64_t *bars = reinterpret_cast<uint64_t *>(sRed + 2 * 3 * 128 * 3);
+  float *sRed = reinterpret_cast<float *>(sWo + 256);  // [2][kFusedParts-1][128][3] partial outputs
+  uint64_t *bars = reinterpret_cast<uint64_t *>(sRed + 2 * (kFusedParts - 1) * 128 * 3);
   uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 60);
   const uint32_t sA_u = smem_u32(sA), sB_u = smem_u32(sB), bars_u = smem_u32(bars);
   auto a_full = [&](int s) { return bars_u + 8u * s; };
@@ -1124,7 +1125,7 @@ __global__ void __launch_bounds__(kFusedWarps * 32, 1)
     __syncwarp();
   } else if (warp >= 4) {
     // ---- epilogue: warp w drains TMEM lanes 32*(w%4).. (the lanes it may
-    // access) and the 32-column chunks part, part+4, ... of them
+    // access) and the 32-column chunks part, part + kFusedParts, ... of them
     const int q = warp & 3, part = (warp - 4) >> 2;
     unsigned char *my_stage = sStage + (warp - 4) * 2048;  // one staging tile per warp
     int pend = -1;    // lane 0: tile whose stores are issued but not yet signalled
@@ -1196,7 +1197,7 @@ __global__ void __launch_bounds__(kFusedWarps * 32, 1)
           };
           (void)chunks;
           uint32_t va[32];
-          for (int c = part; c < N / 32; c += 4) {
+          for (int c = part; c < N / 32; c += kFusedParts) {
             tmem_ld32(va, tbase + c * 32);
             tmem_wait();
             emit(va, c * 32);
@@ -1208,7 +1209,7 @@ __global__ void __launch_bounds__(kFusedWarps * 32, 1)
           // partial sums in part order through sRed, and part 0 writes Y
           float acc[kFusedMaxOut] = {0.0f, 0.0f, 0.0f};
           uint32_t va[32];
-          for (int c = part; c < N / 32; c += 4) {
+          for (int c = part; c < N / 32; c += kFusedParts) {
             tmem_ld32(va, tbase + c * 32);
             tmem_wait();
             fused_gelu_fold32(va, c * 32, bias, sWo, acc);
@@ -1216,7 +1217,7 @@ __global__ void __launch_bounds__(kFusedWarps * 32, 1)
           const int ob = otile & 1;
           const int row = q * 32 + lane;
           if (part > 0) {
-            float *r = sRed + (((ob * 3) + part - 1) * 128 + row) * 3;
+            float *r = sRed + (((ob * (kFusedParts - 1)) + part - 1) * 128 + row) * 3;
             r[0] = acc[0];
             r[1] = acc[1];
             r[2] = acc[2];
@@ -1233,7 +1234,8 @@ __global__ void __launch_bounds__(kFusedWarps * 32, 1)
               for (int o = 0; o < kFusedMaxOut; ++o) {
                 float sum = acc[o];
 #pragma unroll
-                for (int pp = 0; pp < 3; ++pp) sum += sRed[(((ob * 3) + pp) * 128 + row) * 3 + o];
+                for (int pp = 0; pp < kFusedParts - 1; ++pp)
+                  sum += sRed[(((ob * (kFusedParts - 1)) + pp) * 128 + row) * 3 + o];
                 if (o < f.out_dim) y[o] = sum + bo[o];
               }
             }
@@ -1846,7 +1848,7 @@ int fused_predict(mcml_mlp *p, const float *X, uint64_t n, float *mean, float *s
   // barriers, TMEM slot, 1 KB of alignment slack
   const size_t fixed =
       tc_align1k((size_t)maxB) + kFusedEpiWarps * 2048 + 3 * 256 * 4 + 256 * 16 +
-      2 * 3 * 128 * 3 * 4 + 60 * 8 + 16 + 1024;
+      2 * (kFusedParts - 1) * 128 * 3 * 4 + 60 * 8 + 16 + 1024;
   const size_t slot = tc_slot_bytes(64);
   f.slots = (int)std::min<size_t>(16, (kTcSmemMax - fixed) / slot);
   if (f.slots < 2) return set_error(MCML_E_INVALID, "mlp: layers too wide for the fused forward");
