@@ -200,7 +200,8 @@ def test_pipeline_wait_timeout_is_reported_and_drained(gpu_available, monkeypatc
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("hidden,depth,n", [(256, 4, 3000), (64, 3, 1000), (128, 2, 70000),
-                                            (256, 1, 5000)])  # depth 1: the output folded into layer 0
+                                            (256, 1, 5000),   # depth 1: the output folded into layer 0
+                                            (192, 2, 9000)])  # six 32-column chunks over four warps
 def test_fused_forward_agrees_with_layer_by_layer(hidden, depth, n, gpu_available, monkeypatch):
     """With a hidden width that is a multiple of 64 and MCML_MLP_FUSED=1,
     predict() runs every layer of every member in one launch (the fused
