@@ -1500,16 +1500,42 @@ __global__ void narrow_back_kernel(const bf16 *dZ, int ld_dz, long long stride_d
                                    long long strideW, int fo, const float *Z, int ldz,
                                    long long strideZ, bf16 *dH, int ldh, long long strideH, int n,
                                    int fi) {
+  // thread j: hidden unit j (fi <= blockDim.x), its fo weights held in
+  // registers when fo <= 4; blocks stride over the rows, four at a time
   const int zm = blockIdx.z;
-  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= (long long)n * fi) return;
-  const int r = (int)(e / fi), j = (int)(e % fi);
-  const bf16 *dz = dZ + zm * stride_dz + (long long)r * ld_dz;
+  const int j = threadIdx.x;
+  if (j >= fi) return;
   const bf16 *w = W + zm * strideW + (long long)j * fo;
-  float acc = 0.0f;
-  for (int o = 0; o < fo; ++o) acc = fmaf(__bfloat162float(dz[o]), __bfloat162float(w[o]), acc);
-  const float zz = Z[zm * strideZ + (long long)r * ldz + j];
-  dH[zm * strideH + (long long)r * ldh + j] = __float2bfloat16(acc * gelu_grad(zz));
+  const bf16 *dzm = dZ + zm * stride_dz;
+  const float *Zm = Z + zm * strideZ;
+  bf16 *dHm = dH + zm * strideH;
+  if (fo <= 4) {
+    float wr[4];
+#pragma unroll
+    for (int o = 0; o < 4; ++o) wr[o] = o < fo ? __bfloat162float(w[o]) : 0.0f;
+    for (int r0 = blockIdx.x * 4; r0 < n; r0 += gridDim.x * 4) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int r = r0 + i;
+        if (r >= n) break;
+        const bf16 *dz = dzm + (long long)r * ld_dz;
+        float acc = 0.0f;
+#pragma unroll
+        for (int o = 0; o < 4; ++o)
+          if (o < fo) acc = fmaf(__bfloat162float(dz[o]), wr[o], acc);
+        const float zz = Zm[(long long)r * ldz + j];
+        dHm[(long long)r * ldh + j] = __float2bfloat16(acc * gelu_grad(zz));
+      }
+    }
+    return;
+  }
+  for (int r = blockIdx.x; r < n; r += gridDim.x) {
+    const bf16 *dz = dzm + (long long)r * ld_dz;
+    float acc = 0.0f;
+    for (int o = 0; o < fo; ++o) acc = fmaf(__bfloat162float(dz[o]), __bfloat162float(w[o]), acc);
+    const float zz = Zm[(long long)r * ldz + j];
+    dHm[(long long)r * ldh + j] = __float2bfloat16(acc * gelu_grad(zz));
+  }
 }
 
 // Adam on the FP32 master weights; refreshes the BF16 mirror.
@@ -1982,11 +2008,12 @@ int backward(mcml_mlp *p, int n) {
       dcur_ld = H;
       continue;
     }
-    narrow_back_kernel<<<dim3((unsigned)(((long long)n * fi + 255) / 256), 1, p->E), 256, 0,
-                         p->stream>>>(dcur, dcur_ld, cap * std::max<long long>(H, p->out_dim),
-                                      p->d_w16 + p->w_off[l], P, fo,
-                                      p->d_z + (long long)(l - 1) * cap * H, (int)H, D * cap * H,
-                                      dnext, (int)H, cap * std::max<long long>(H, p->out_dim), n, fi);
+    // one thread per hidden unit (fi <= 256), blocks striding over the rows
+    narrow_back_kernel<<<dim3((unsigned)std::min((n + 3) / 4, 1024), 1, p->E), 256, 0,
+                         p->stream>>>(
+        dcur, dcur_ld, cap * std::max<long long>(H, p->out_dim), p->d_w16 + p->w_off[l], P, fo,
+        p->d_z + (long long)(l - 1) * cap * H, (int)H, D * cap * H, dnext, (int)H,
+        cap * std::max<long long>(H, p->out_dim), n, fi);
     MLP_TRY(cudaGetLastError());
     std::swap(dcur, dnext);
     dcur_ld = H;
